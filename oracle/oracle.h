@@ -1,0 +1,152 @@
+/*
+ * CPU oracle for the peak-group-selection path — TEST INFRASTRUCTURE ONLY.
+ *
+ * A from-scratch C++17 restatement of the reference crate's scalar CPU path
+ * (MannLabs/alphadia-search-rs).  Only tests, `__graft_entry__.smoke()` and the
+ * CPU legs of `bench.py` may load it, and only as the checker or the timed CPU
+ * baseline.  The product (libads_gpu.so) never links or calls it.
+ *
+ * Every function cites the reference file:line it restates.  Arithmetic is
+ * plain IEEE f32 in the reference's operation order; the library is compiled
+ * with -ffp-contract=off and without fast-math so no FMA contraction or
+ * re-association happens, and it calls glibc logf/expf/sqrtf exactly where the
+ * reference calls f32::ln/exp/sqrt (Rust lowers those to the platform libm).
+ *
+ * Parity pin: the known-answer tests of the reference crate for this path
+ * (grid length, RT limits, window membership, builder ordering, XIC sums,
+ * log-dot values, local maxima, fragment filter, candidate arrays) are ported
+ * as tests against this library.  No reference test pins an end-to-end
+ * search() result; the whole-path result is pinned only piecewise.
+ */
+#ifndef ADS_ORACLE_H
+#define ADS_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- m/z grid: src/mz_index/mod.rs:8-25, :55-90, :95-127 ---- */
+int64_t orc_ppm_index_len(float resolution_ppm, float mz_start, float mz_end);
+/* writes orc_ppm_index_len(...) values */
+void orc_ppm_index(float resolution_ppm, float mz_start, float mz_end, float* out);
+int64_t orc_find_closest_index(const float* grid, int64_t n, float mz);
+void orc_mz_range_indices(const float* grid, int64_t n, float lower_mz, float upper_mz,
+                          int64_t* start, int64_t* stop);
+
+/* ---- RT index: src/rt_index/mod.rs:20-26, :89-138 ---- */
+float orc_mean_delta_t(const float* rt, int64_t n);
+void orc_rt_limits(const float* rt, int64_t n, float delta_t, float precursor_rt,
+                   float rt_tolerance, int64_t num_cycles_padding, int64_t* lower, int64_t* upper);
+
+/* Rust 1.88 `slice::binary_search` on sorted u16 values (returns Ok/Err index). */
+int64_t orc_rust_binary_search_u16(const uint16_t* a, int64_t n, uint16_t x);
+
+/* ---- Gaussian kernel: src/kernel/mod.rs:13-56; returns the array length ---- */
+int64_t orc_gaussian_kernel(float fwhm_rt, float sigma_scale_rt, int64_t kernel_width,
+                            float rt_resolution, float* out /* capacity >= kernel_width + 2 */);
+
+/* ---- convolution: src/convolution/scalar.rs:5-56 ---- */
+void orc_convolution(const float* kernel, int64_t klen, const float* xic, int64_t n_rows,
+                     int64_t n_cols, float* out);
+
+/* ---- log-dot score: src/score/scalar.rs:4-25.
+ * log_mode 0: glibc logf (what the reference calls on Linux).
+ * log_mode 1: logf correctly rounded, i.e. (float)log((double)x). ---- */
+void orc_log_dot(const float* a, int64_t n_rows, int64_t n_cols, const float* w, float* out,
+                 int log_mode);
+
+/* ---- local maxima: src/peak_group_selection/mod.rs:23-64; returns the count ---- */
+int64_t orc_local_maxima(const float* a, int64_t n, int64_t offset, int64_t* idx, float* val);
+
+/* ---- fragment filter: src/speclib_flat/mod.rs:240-345.
+ * Writes the original positions of the kept fragments in output order and
+ * returns how many were kept. ---- */
+int64_t orc_filter_sort_fragments(int64_t n, const float* mz, const float* intensity,
+                                  const uint8_t* number, const uint8_t* type, int non_zero,
+                                  int filter_y1, int64_t top_k, int64_t* out_pos);
+
+/* ---- DIAData build: src/dia_data_builder/mod.rs:11-139, src/rt_index/mod.rs:53-75 ---- */
+typedef struct OrcDia OrcDia;
+OrcDia* orc_dia_build(int64_t n_spectra, const int64_t* delta_scan_idx, const float* iso_lower,
+                      const float* iso_upper, const int64_t* peak_start, const int64_t* peak_stop,
+                      const int64_t* cycle_idx, const float* spectrum_rt, int64_t n_peaks,
+                      const float* peak_mz, const float* peak_intensity, int n_threads);
+void orc_dia_free(OrcDia* d);
+int64_t orc_dia_num_obs(const OrcDia* d);
+int64_t orc_dia_grid_len(const OrcDia* d);
+const float* orc_dia_grid(const OrcDia* d);
+int64_t orc_dia_rt_len(const OrcDia* d);
+const float* orc_dia_rt(const OrcDia* d);
+float orc_dia_delta_t(const OrcDia* d);
+void orc_dia_obs_window(const OrcDia* d, int64_t obs, float* lower, float* upper);
+int64_t orc_dia_obs_num_cycles(const OrcDia* d, int64_t obs);
+int64_t orc_dia_obs_num_peaks(const OrcDia* d, int64_t obs);
+const uint32_t* orc_dia_obs_slice_starts(const OrcDia* d, int64_t obs);
+const uint16_t* orc_dia_obs_cycles(const OrcDia* d, int64_t obs);
+const float* orc_dia_obs_intensities(const OrcDia* d, int64_t obs);
+/* src/quadrupole_observation/mod.rs:70-107 on a caller-built observation
+ * (slice_starts has n_slices+1 entries); adds into xic[stop-start]. */
+void orc_fill_xic_slice_raw(const uint32_t* slice_starts, int64_t n_slices, const uint16_t* cycles,
+                            const float* intensities, const float* grid, int64_t grid_len,
+                            float* xic, int64_t cycle_start, int64_t cycle_stop,
+                            float mass_tolerance, float mz);
+/* src/dia_data/mod.rs:79-87; returns count, writes up to cap indices */
+int64_t orc_dia_valid_observations(const OrcDia* d, float precursor_mz, int64_t* out, int64_t cap);
+/* src/dense_xic_observation/mod.rs:30-64 — out is n_frag x (stop-start), row-major */
+void orc_dense_xic(const OrcDia* d, float precursor_mz, int64_t cycle_start, int64_t cycle_stop,
+                   float mass_tolerance, const float* fragment_mz, int64_t n_frag, float* out);
+
+/* ---- SpecLibFlat: src/speclib_flat/mod.rs:100-188 (stable sort by precursor_idx) ---- */
+typedef struct OrcLib OrcLib;
+OrcLib* orc_lib_build(int64_t n_prec, const uint64_t* precursor_idx, const float* precursor_mz,
+                      const float* precursor_rt, const uint64_t* frag_start,
+                      const uint64_t* frag_stop, int64_t n_frag, const float* fragment_mz,
+                      const float* fragment_intensity, const uint8_t* fragment_number,
+                      const uint8_t* fragment_type);
+void orc_lib_free(OrcLib* l);
+int64_t orc_lib_num_precursors(const OrcLib* l);
+
+/* ---- search: src/peak_group_selection/mod.rs:94-195 ---- */
+typedef struct {
+  float fwhm_rt;
+  int64_t kernel_size;
+  int64_t peak_length;
+  float mass_tolerance;
+  float rt_tolerance;
+  int64_t candidate_count;
+  int64_t top_k_fragments;
+} OrcParams;
+
+typedef struct OrcResult OrcResult;
+/* rt_tolerance_per_precursor: optional (NULL = params.rt_tolerance for all), indexed in
+ * sorted-library order.  subset: optional list of sorted-library positions to search
+ * (NULL = all, in order).  precision 0 = f32 (reference), 1 = f64 variant (same control
+ * flow, XIC/kernel/convolution/log/score in double). */
+OrcResult* orc_search(const OrcDia* d, const OrcLib* l, const OrcParams* p,
+                      const float* rt_tolerance_per_precursor, const int64_t* subset,
+                      int64_t n_subset, int log_mode, int precision, int n_threads);
+int64_t orc_result_len(const OrcResult* r);
+void orc_result_copy(const OrcResult* r, uint64_t* precursor_idx, uint64_t* rank, float* score,
+                     double* score_f64, uint64_t* cycle_center, uint64_t* cycle_start,
+                     uint64_t* cycle_stop);
+void orc_result_free(OrcResult* r);
+
+/* Per-precursor trace for debugging: fills the filtered fragment count, the cycle
+ * limits and (if the buffers are large enough) the XIC, convolved XIC and score. */
+int64_t orc_trace_precursor(const OrcDia* d, const OrcLib* l, const OrcParams* p,
+                            float rt_tolerance, int64_t lib_pos, int log_mode,
+                            int64_t* cycle_start, int64_t* cycle_stop, int64_t* n_frag,
+                            float* xic, float* conv, float* score, int64_t cap);
+
+/* f64 score of one precursor at given absolute cycles (for BF16 error reports). Writes
+ * scores and returns max_j |score_f64[j]| over the whole cycle window. */
+double orc_scores_f64_at(const OrcDia* d, const OrcLib* l, const OrcParams* p,
+                         float rt_tolerance, int64_t lib_pos, const int64_t* cycles, int64_t n,
+                         double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
