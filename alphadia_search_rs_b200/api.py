@@ -1,0 +1,591 @@
+"""Python classes with the reference module's names and behaviour.
+
+Mirrors the pyo3 classes of MannLabs/alphadia-search-rs (src/lib.rs:74-93) that
+the selection path uses: ``DIAData``, ``SpecLibFlat``, ``SelectionParameters``,
+``PeakGroupSelection`` and ``CandidateCollection``.  Every call goes through the
+C ABI of ``include/ads_gpu.h``; the work runs on the GPU.  Extensions beyond the
+reference API are keyword-only arguments with defaults that keep the reference
+behaviour.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Any
+
+import numpy as np
+
+from . import _ffi as F
+
+_DEFAULT_DEVICE = 0
+
+
+def _lib():
+    return F.load()
+
+
+def _is_device_tensor(x: Any) -> bool:
+    return hasattr(x, "is_cuda") and bool(getattr(x, "is_cuda"))
+
+
+def _as_np(name: str, x: Any, dtype) -> np.ndarray:
+    """numpy view of ``x`` with exactly ``dtype`` (pyo3's PyReadonlyArray1<T>
+    rejects other dtypes with TypeError)."""
+    if not isinstance(x, np.ndarray):
+        raise TypeError(f"argument '{name}': expected numpy.ndarray of {np.dtype(dtype).name}, got {type(x).__name__}")
+    if x.dtype != np.dtype(dtype):
+        raise TypeError(f"argument '{name}': expected dtype {np.dtype(dtype).name}, got {x.dtype.name}")
+    return np.ascontiguousarray(x)
+
+
+def _dev_ptr(name: str, t: Any, dtype, device: int) -> int:
+    import torch
+
+    want = {np.float32: torch.float32, np.int64: torch.int64, np.uint8: torch.uint8,
+            np.uint64: torch.uint64}[dtype]
+    if t.dtype != want:
+        raise TypeError(f"argument '{name}': expected dtype {want}, got {t.dtype}")
+    if t.device.index != device:
+        raise ValueError(f"argument '{name}': tensor on cuda:{t.device.index}, expected cuda:{device}")
+    if not t.is_contiguous():
+        raise ValueError(f"argument '{name}': tensor must be contiguous")
+    return int(t.data_ptr())
+
+
+class DIAData:
+    """DIAData (src/dia_data/mod.rs:15-136), device resident."""
+
+    def __init__(self):
+        self._h = None
+        self._n_obs = 0
+        self._iso = np.zeros((0, 2), np.float32)
+        self._num_peaks = np.zeros(0, np.int64)
+        self._rt_values = np.zeros(0, np.float32)
+        self._cycle = np.zeros((0, 0, 0, 0), np.float32)
+        self.device = _DEFAULT_DEVICE
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                _lib().ads_dia_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @staticmethod
+    def from_arrays(spectrum_delta_scan_idx, isolation_lower_mz, isolation_upper_mz,
+                    spectrum_peak_start_idx, spectrum_peak_stop_idx, spectrum_cycle_idx,
+                    spectrum_rt, peak_mz, peak_intensity, cycle, *, device: int | None = None):
+        """DIAData::from_arrays (src/dia_data/mod.rs:41-72).  The first nine arrays
+        may instead all be CUDA tensors on ``device`` (same dtypes)."""
+        L = _lib()
+        names = ["spectrum_delta_scan_idx", "isolation_lower_mz", "isolation_upper_mz",
+                 "spectrum_peak_start_idx", "spectrum_peak_stop_idx", "spectrum_cycle_idx",
+                 "spectrum_rt", "peak_mz", "peak_intensity"]
+        dtypes = [np.int64, np.float32, np.float32, np.int64, np.int64, np.int64, np.float32,
+                  np.float32, np.float32]
+        arrays = [spectrum_delta_scan_idx, isolation_lower_mz, isolation_upper_mz,
+                  spectrum_peak_start_idx, spectrum_peak_stop_idx, spectrum_cycle_idx,
+                  spectrum_rt, peak_mz, peak_intensity]
+        cyc = _as_np("cycle", cycle, np.float32)
+        if cyc.ndim != 4:
+            raise TypeError("argument 'cycle': expected a 4-D float32 array")
+        on_dev = [_is_device_tensor(a) for a in arrays]
+        if any(on_dev) and not all(on_dev):
+            raise ValueError("spectrum and peak arrays must be all host arrays or all CUDA tensors")
+        raw = F.AdsRawArrays()
+        keep = []
+        if all(on_dev):
+            dev = arrays[0].device.index if device is None else device
+            raw.location = F.ADS_MEM_DEVICE
+            ptrs = [_dev_ptr(n, a, t, dev) for n, a, t in zip(names, arrays, dtypes)]
+            lens = [int(a.numel()) for a in arrays]
+        else:
+            dev = _DEFAULT_DEVICE if device is None else device
+            raw.location = F.ADS_MEM_HOST
+            np_arrays = [_as_np(n, a, t) for n, a, t in zip(names, arrays, dtypes)]
+            keep.extend(np_arrays)
+            ptrs = [a.ctypes.data for a in np_arrays]
+            lens = [a.size for a in np_arrays]
+        n_spec = lens[0]
+        if any(n != n_spec for n in lens[1:7]):
+            raise ValueError("spectrum arrays must have the same length")
+        if lens[7] != lens[8]:
+            raise ValueError("peak_mz and peak_intensity must have the same length")
+        raw.n_spectra = n_spec
+        (raw.spectrum_delta_scan_idx, raw.isolation_lower_mz, raw.isolation_upper_mz,
+         raw.spectrum_peak_start_idx, raw.spectrum_peak_stop_idx, raw.spectrum_cycle_idx,
+         raw.spectrum_rt, raw.peak_mz, raw.peak_intensity) = ptrs
+        raw.n_peaks = lens[7]
+        raw.cycle = cyc.ctypes.data if cyc.size else None
+        for i in range(4):
+            raw.cycle_shape[i] = cyc.shape[i]
+        h = C.c_void_p()
+        F.check(L.ads_dia_create(C.byref(raw), int(dev), C.byref(h)))
+        d = DIAData()
+        d._h = h.value
+        d.device = int(dev)
+        d._load_meta()
+        return d
+
+    def _load_meta(self):
+        L = _lib()
+        self._n_obs = int(L.ads_dia_num_observations(self._h))
+        iso = np.zeros((self._n_obs, 2), np.float32)
+        npk = np.zeros(self._n_obs, np.int64)
+        lo, hi, nc, n = C.c_float(), C.c_float(), C.c_int64(), C.c_int64()
+        for w in range(self._n_obs):
+            F.check(L.ads_dia_observation_info(self._h, w, C.byref(lo), C.byref(hi), C.byref(nc), C.byref(n)))
+            iso[w] = (lo.value, hi.value)
+            npk[w] = n.value
+        self._iso, self._num_peaks = iso, npk
+        cnt = C.c_int64()
+        F.check(L.ads_dia_rt_values(self._h, None, 0, C.byref(cnt)))
+        rtv = np.zeros(max(cnt.value, 1), np.float32)
+        F.check(L.ads_dia_rt_values(self._h, rtv.ctypes.data, cnt.value, C.byref(cnt)))
+        self._rt_values = rtv[:cnt.value].copy()
+        shape = (C.c_int64 * 4)()
+        F.check(L.ads_dia_cycle(self._h, None, 0, C.byref(shape)))
+        cyc = np.zeros(tuple(shape), np.float32)
+        if cyc.size:
+            F.check(L.ads_dia_cycle(self._h, cyc.ctypes.data, cyc.size, C.byref(shape)))
+        self._cycle = cyc
+
+    # ---- getters (src/dia_data/mod.rs:74-135)
+    @property
+    def num_observations(self) -> int:
+        return self._n_obs
+
+    def get_valid_observations(self, precursor_mz: float) -> list[int]:
+        """src/dia_data/mod.rs:79-87: windows with lower <= mz <= upper, in order."""
+        mz = np.float32(precursor_mz)
+        return [i for i in range(self._n_obs) if self._iso[i, 0] <= mz and self._iso[i, 1] >= mz]
+
+    def memory_footprint_bytes(self) -> int:
+        return int(_lib().ads_dia_memory_footprint_bytes(self._h)) if self._h else 24
+
+    def memory_footprint_mb(self) -> float:
+        return self.memory_footprint_bytes() / (1024.0 * 1024.0)
+
+    @property
+    def has_mobility(self) -> bool:
+        return False
+
+    @property
+    def has_ms1(self) -> bool:
+        return False
+
+    @property
+    def mobility_values(self) -> list[float]:
+        return [1e-6, 0.0]
+
+    @property
+    def rt_values(self) -> np.ndarray:
+        return self._rt_values.copy()
+
+    @property
+    def cycle(self) -> np.ndarray:
+        return self._cycle.copy()
+
+    # ---- engine extras
+    def rt_index(self) -> tuple[np.ndarray, float]:
+        L = _lib()
+        n, dt = C.c_int64(), C.c_float()
+        F.check(L.ads_dia_rt_index(self._h, None, 0, C.byref(n), C.byref(dt)))
+        out = np.zeros(max(n.value, 1), np.float32)
+        F.check(L.ads_dia_rt_index(self._h, out.ctypes.data, n.value, C.byref(n), C.byref(dt)))
+        return out[:n.value].copy(), float(dt.value)
+
+    def observation(self, obs: int) -> dict:
+        """CSR of one quadrupole observation copied to host (slice_starts,
+        cycle_indices, intensities)."""
+        L = _lib()
+        g = int(L.ads_mz_grid_len())
+        n = int(self._num_peaks[obs])
+        ss = np.zeros(g + 1, np.uint32)
+        cy = np.zeros(max(n, 1), np.uint16)
+        it = np.zeros(max(n, 1), np.float32)
+        F.check(L.ads_dia_copy_observation(self._h, obs, ss.ctypes.data, cy.ctypes.data, it.ctypes.data))
+        return dict(isolation_window=tuple(self._iso[obs]), slice_starts=ss,
+                    cycle_indices=cy[:n], intensities=it[:n])
+
+
+class SpecLibFlat:
+    """SpecLibFlat (src/speclib_flat/mod.rs:6-199), device resident."""
+
+    def __init__(self):
+        self._h = None
+        self._n_prec = 0
+        self._n_frag = 0
+        self.device = _DEFAULT_DEVICE
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                _lib().ads_lib_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @staticmethod
+    def from_arrays(precursor_idx, precursor_mz_library, precursor_mz, precursor_rt_library,
+                    precursor_rt, precursor_naa, flat_frag_start_idx, flat_frag_stop_idx,
+                    fragment_mz_library, fragment_mz, fragment_intensity, fragment_cardinality,
+                    fragment_charge, fragment_loss_type, fragment_number, fragment_position,
+                    fragment_type, *, precursor_rt_tolerance=None, device: int | None = None):
+        """SpecLibFlat::from_arrays (src/speclib_flat/mod.rs:98-188).
+        ``precursor_rt_tolerance`` (extension): per-precursor RT half-window in
+        seconds replacing SelectionParameters.rt_tolerance."""
+        L = _lib()
+        spec = [("precursor_idx", precursor_idx, np.uint64), ("precursor_mz_library", precursor_mz_library, np.float32),
+                ("precursor_mz", precursor_mz, np.float32), ("precursor_rt_library", precursor_rt_library, np.float32),
+                ("precursor_rt", precursor_rt, np.float32), ("precursor_naa", precursor_naa, np.uint8),
+                ("flat_frag_start_idx", flat_frag_start_idx, np.uint64), ("flat_frag_stop_idx", flat_frag_stop_idx, np.uint64),
+                ("fragment_mz_library", fragment_mz_library, np.float32), ("fragment_mz", fragment_mz, np.float32),
+                ("fragment_intensity", fragment_intensity, np.float32), ("fragment_cardinality", fragment_cardinality, np.uint8),
+                ("fragment_charge", fragment_charge, np.uint8), ("fragment_loss_type", fragment_loss_type, np.uint8),
+                ("fragment_number", fragment_number, np.uint8), ("fragment_position", fragment_position, np.uint8),
+                ("fragment_type", fragment_type, np.uint8)]
+        if precursor_rt_tolerance is not None:
+            spec.append(("precursor_rt_tolerance", precursor_rt_tolerance, np.float32))
+        on_dev = [_is_device_tensor(a) for _, a, _ in spec]
+        if any(on_dev) and not all(on_dev):
+            raise ValueError("library arrays must be all host arrays or all CUDA tensors")
+        arr = F.AdsLibArrays()
+        keep = []
+        if all(on_dev):
+            dev = spec[0][1].device.index if device is None else device
+            arr.location = F.ADS_MEM_DEVICE
+            ptr = {n: _dev_ptr(n, a, t, dev) for n, a, t in spec}
+            lens = {n: int(a.numel()) for n, a, _ in spec}
+        else:
+            dev = _DEFAULT_DEVICE if device is None else device
+            arr.location = F.ADS_MEM_HOST
+            conv = {n: _as_np(n, a, t) for n, a, t in spec}
+            keep.append(conv)
+            ptr = {n: a.ctypes.data for n, a in conv.items()}
+            lens = {n: a.size for n, a in conv.items()}
+        n_prec = lens["precursor_idx"]
+        n_frag = lens["fragment_mz"]
+        for n, _, _ in spec:
+            want = n_prec if n.startswith("precursor") or n.startswith("flat") else n_frag
+            if lens[n] != want:
+                raise ValueError(f"argument '{n}': length {lens[n]}, expected {want}")
+        arr.n_precursors = n_prec
+        arr.n_fragments = n_frag
+        for n, _, _ in spec:
+            setattr(arr, n, ptr[n] if lens[n] else None)
+        h = C.c_void_p()
+        F.check(L.ads_lib_create(C.byref(arr), int(dev), C.byref(h)))
+        lib = SpecLibFlat()
+        lib._h = h.value
+        lib._n_prec = n_prec
+        lib._n_frag = n_frag
+        lib.device = int(dev)
+        return lib
+
+    @property
+    def num_precursors(self) -> int:
+        return self._n_prec
+
+    @property
+    def num_fragments(self) -> int:
+        return self._n_frag
+
+
+_FLOAT_KEYS = ("fwhm_rt", "mass_tolerance", "rt_tolerance")
+_USIZE_KEYS = ("kernel_size", "peak_length", "candidate_count", "top_k_fragments")
+
+
+class SelectionParameters:
+    """SelectionParameters (src/peak_group_selection/parameters.rs:4-75): read-only
+    attributes, defaults of ``new``, and ``update(dict)``."""
+
+    __slots__ = ("_v",)
+
+    def __init__(self):
+        p = F.AdsSelectionParams()
+        _lib().ads_selection_params_default(C.byref(p))
+        object.__setattr__(self, "_v", {k: getattr(p, k) for k, _ in F.AdsSelectionParams._fields_})
+        for k in _FLOAT_KEYS:
+            self._v[k] = float(np.float32(self._v[k]))
+
+    def __getattr__(self, name):
+        v = object.__getattribute__(self, "_v")
+        if name in v:
+            return v[name]
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        raise AttributeError(f"attribute '{name}' of 'SelectionParameters' objects is not writable")
+
+    def update(self, config: dict) -> None:
+        """Sets any of the seven keys present in ``config`` (parameters.rs:45-68)."""
+        new = dict(self._v)
+        for k in _FLOAT_KEYS:
+            if k in config:
+                val = config[k]
+                if isinstance(val, (bool, np.bool_)) or not isinstance(val, (int, float, np.integer, np.floating)):
+                    if not hasattr(val, "__float__"):
+                        raise TypeError(f"'{type(val).__name__}' object cannot be converted to 'PyFloat'")
+                new[k] = float(np.float32(float(val)))
+        for k in _USIZE_KEYS:
+            if k in config:
+                val = config[k]
+                if isinstance(val, (float, np.floating)) or not hasattr(val, "__index__"):
+                    raise TypeError(f"'{type(val).__name__}' object cannot be interpreted as an integer")
+                iv = int(val.__index__())
+                if iv < 0:
+                    raise OverflowError("can't convert negative int to unsigned")
+                if iv >= 2**64:
+                    raise OverflowError("int too big to convert")
+                new[k] = iv
+        object.__setattr__(self, "_v", new)
+
+    def _c(self) -> F.AdsSelectionParams:
+        p = F.AdsSelectionParams()
+        for k, _ in F.AdsSelectionParams._fields_:
+            v = self._v[k]
+            if k in _USIZE_KEYS:
+                v = min(v, 2**63 - 1)
+            setattr(p, k, v)
+        return p
+
+    def __repr__(self):
+        return "SelectionParameters(" + ", ".join(f"{k}={v!r}" for k, v in self._v.items()) + ")"
+
+
+class CandidateCollection:
+    """CandidateCollection (src/candidate/entry.rs:41-193)."""
+
+    _COLS = ("precursor_idx", "rank", "score", "scan_center", "scan_start", "scan_stop",
+             "cycle_center", "cycle_start", "cycle_stop")
+
+    def __init__(self):
+        self._h = None
+        self._arrays = {c: np.zeros(0, np.float32 if c == "score" else np.uint64) for c in self._COLS}
+        self._n = 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                _lib().ads_candidates_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @classmethod
+    def _from_handle(cls, h: int) -> "CandidateCollection":
+        c = cls()
+        c._h = h
+        n = int(_lib().ads_candidates_size(h))
+        if n < 0:
+            F.check(F.ADS_ERR_INTERNAL)
+        c._n = n
+        c._arrays = None
+        return c
+
+    def _materialize(self) -> dict:
+        if self._arrays is None:
+            n = self._n
+            cols = {c: np.zeros(n, np.float32 if c == "score" else np.uint64) for c in self._COLS}
+            if n:
+                ptr = [cols[c].ctypes.data for c in self._COLS]
+                for i in (3, 4, 5):  # scan_* stay zero (np.zeros), as in the reference
+                    ptr[i] = None
+                F.check(_lib().ads_candidates_copy_out(self._h, *ptr))
+            self._arrays = cols
+            _lib().ads_candidates_destroy(self._h)
+            self._h = None
+        return self._arrays
+
+    @staticmethod
+    def from_arrays(precursor_idxs, ranks, scores, scan_center, scan_start, scan_stop,
+                    cycle_center, cycle_start, cycle_stop) -> "CandidateCollection":
+        """src/candidate/entry.rs:70-120 (ValueError when lengths differ)."""
+        cols = [precursor_idxs, ranks, scores, scan_center, scan_start, scan_stop, cycle_center,
+                cycle_start, cycle_stop]
+        n = len(cols[0])
+        if not all(len(c) == n for c in cols[1:]):
+            raise ValueError("All input arrays must have the same length")
+        c = CandidateCollection()
+        c._arrays = {name: np.asarray(v, dtype=np.float32 if name == "score" else np.uint64).copy()
+                     for name, v in zip(CandidateCollection._COLS, cols)}
+        c._n = n
+        return c
+
+    def len(self) -> int:
+        return self._n
+
+    def __len__(self) -> int:
+        return self._n
+
+    def is_empty(self) -> bool:
+        return self._n == 0
+
+    def to_arrays(self, *, out=None):
+        """Nine arrays in the reference's tuple order (src/candidate/entry.rs:124-173):
+        precursor_idx, rank, score, scan_center, scan_start, scan_stop, cycle_center,
+        cycle_start, cycle_stop.
+
+        ``out`` (extension): nine preallocated arrays (for example views of pinned
+        memory) of at least len() elements; the first len() entries are written and
+        views of them returned."""
+        if out is not None and self._h is not None and self._arrays is None:
+            n = self._n
+            if len(out) != 9 or any(len(o) < n for o in out):
+                raise ValueError("out must be nine arrays of at least len() elements")
+            for o, c in zip(out, self._COLS):
+                want = np.float32 if c == "score" else np.uint64
+                if o.dtype != want or not o.flags.c_contiguous:
+                    raise TypeError(f"out array for {c} must be contiguous {np.dtype(want).name}")
+            if n:
+                F.check(_lib().ads_candidates_copy_out(self._h, *[o.ctypes.data for o in out]))
+            return tuple(o[:n] for o in out)
+        a = self._materialize()
+        return tuple(a[c].copy() for c in self._COLS)
+
+
+class PeakGroupSelection:
+    """PeakGroupSelection (src/peak_group_selection/mod.rs:66-90) on the GPU."""
+
+    def __init__(self, params: SelectionParameters, *, precision: str = "fp32", verbose: bool = True,
+                 device: int | None = None, warps_per_block: int = 0, blocks_per_sm: int = 0,
+                 gather_mode: int = 0, time_stages: bool = False, stream: int = 0):
+        if not isinstance(params, SelectionParameters):
+            raise TypeError("argument 'params': expected SelectionParameters")
+        L = _lib()
+        self.params = params
+        self.device = _DEFAULT_DEVICE if device is None else int(device)
+        o = F.AdsEngineOptions()
+        L.ads_engine_options_default(C.byref(o))
+        o.precision = {"fp32": F.ADS_PRECISION_FP32, "bf16": F.ADS_PRECISION_BF16}[precision]
+        o.verbose = 1 if verbose else 0
+        o.warps_per_block = warps_per_block
+        o.blocks_per_sm = blocks_per_sm
+        o.gather_mode = gather_mode
+        o.time_stages = 1 if time_stages else 0
+        o.stream = int(stream)
+        self._opts = o
+        p = params._c()
+        h = C.c_void_p()
+        F.check(L.ads_selection_create(C.byref(p), C.byref(o), self.device, C.byref(h)))
+        self._h = h.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                _lib().ads_selection_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def search(self, dia_data: DIAData, lib: SpecLibFlat) -> CandidateCollection:
+        if not isinstance(dia_data, DIAData) or not isinstance(lib, SpecLibFlat):
+            raise TypeError("search(dia_data: DIAData, lib: SpecLibFlat)")
+        if dia_data._h is None or lib._h is None:
+            raise ValueError("DIAData and SpecLibFlat must be built with from_arrays")
+        out = C.c_void_p()
+        F.check(_lib().ads_select(self._h, dia_data._h, lib._h, C.byref(out)))
+        return CandidateCollection._from_handle(out.value)
+
+    # ---- engine extras
+    def kernel(self) -> np.ndarray:
+        n = C.c_int64()
+        F.check(_lib().ads_selection_kernel(self._h, None, 0, C.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float32)
+        F.check(_lib().ads_selection_kernel(self._h, out.ctypes.data, n.value, C.byref(n)))
+        return out[:n.value].copy()
+
+    @property
+    def stream(self) -> int:
+        return int(_lib().ads_selection_stream(self._h))
+
+    @property
+    def last_launches(self) -> int:
+        return int(_lib().ads_selection_last_launches(self._h))
+
+    def search_into(self, dia_data: DIAData, lib: SpecLibFlat, cand: "DeviceCandidates") -> None:
+        """Enqueue a search without waiting, reusing ``cand``'s device buffers."""
+        F.check(_lib().ads_select_async(self._h, dia_data._h, lib._h, cand._h))
+
+    def new_candidates(self) -> "DeviceCandidates":
+        return DeviceCandidates(self)
+
+    def stage_times(self) -> dict:
+        """Summed device ms per stage over the searches since the last call
+        (needs time_stages=True)."""
+        out = np.zeros(4, np.float32)
+        F.check(_lib().ads_selection_stage_times(self._h, out.ctypes.data, 4))
+        return dict(prep_ms=float(out[0]), search_ms=float(out[1]), compaction_ms=float(out[2]),
+                    searches=int(out[3]))
+
+    def enable_stats(self, on: bool = True) -> None:
+        F.check(_lib().ads_selection_set_stats(self._h, 1 if on else 0))
+
+    def last_stats(self) -> dict:
+        out = np.zeros(6, np.int64)
+        F.check(_lib().ads_selection_last_stats(self._h, out.ctypes.data, 6))
+        return dict(pairs=int(out[0]), bins_plus_one=int(out[1]), fragments=int(out[2]),
+                    entries_read=int(out[3]), entries_accumulated=int(out[4]),
+                    offsets_read=int(out[5]))
+
+
+class DeviceCandidates:
+    """A reusable device-side candidate buffer for PeakGroupSelection.search_into."""
+
+    def __init__(self, sel: PeakGroupSelection):
+        h = C.c_void_p()
+        F.check(_lib().ads_candidates_create(sel._h, C.byref(h)))
+        self._h = h.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                _lib().ads_candidates_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def size(self) -> int:
+        n = int(_lib().ads_candidates_size(self._h))
+        if n < 0:
+            F.check(F.ADS_ERR_INTERNAL)
+        return n
+
+    def copy_out(self, out: dict) -> int:
+        """Copies into preallocated arrays keyed by column name (missing keys skipped)."""
+        n = self.size()
+        cols = CandidateCollection._COLS
+        ptr = [out[c].ctypes.data if c in out else None for c in cols]
+        F.check(_lib().ads_candidates_copy_out(self._h, *ptr))
+        return n
+
+
+def gaussian_kernel(fwhm_rt: float, sigma_scale_rt: float, kernel_width: int,
+                    rt_resolution: float) -> np.ndarray:
+    """GaussianKernel::new(...).kernel_array (src/kernel/mod.rs:13-56)."""
+    L = _lib()
+    n = C.c_int64()
+    F.check(L.ads_gaussian_kernel(fwhm_rt, sigma_scale_rt, int(kernel_width), rt_resolution, None, 0, C.byref(n)))
+    out = np.zeros(max(n.value, 1), np.float32)
+    F.check(L.ads_gaussian_kernel(fwhm_rt, sigma_scale_rt, int(kernel_width), rt_resolution,
+                                  out.ctypes.data, n.value, C.byref(n)))
+    return out[:n.value].copy()
+
+
+def mz_grid() -> np.ndarray:
+    """The global 1-ppm m/z grid (src/mz_index/mod.rs:4-27)."""
+    L = _lib()
+    n = int(L.ads_mz_grid_len())
+    out = np.zeros(n, np.float32)
+    F.check(L.ads_mz_grid(out.ctypes.data, n))
+    return out
+
+
+def device_count() -> int:
+    return int(_lib().ads_device_count())

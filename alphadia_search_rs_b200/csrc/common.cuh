@@ -1,0 +1,231 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "ads_gpu.h"
+
+namespace ads {
+
+// ------------------------------------------------------------------ errors
+void set_error(const std::string& msg);
+void clear_error();
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define ADS_TRY(expr)                   \
+  do {                                  \
+    int _rc = (expr);                   \
+    if (_rc != ADS_OK) return _rc;      \
+  } while (0)
+
+#define ADS_CUDA(expr)                                                  \
+  do {                                                                  \
+    cudaError_t _e = (expr);                                            \
+    if (_e != cudaSuccess) return ::ads::cuda_fail(_e, #expr, __FILE__, __LINE__); \
+  } while (0)
+
+#define ADS_LAUNCH_CHECK() ADS_CUDA(cudaGetLastError())
+
+// Runs `body` and converts C++ exceptions to status codes so nothing crosses
+// the C boundary.
+template <class F>
+int guarded(F&& body) {
+  try {
+    clear_error();
+    return body();
+  } catch (const std::bad_alloc&) {
+    return fail(ADS_ERR_OUT_OF_MEMORY, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(ADS_ERR_INTERNAL, e.what());
+  } catch (...) {
+    return fail(ADS_ERR_INTERNAL, "unknown exception");
+  }
+}
+
+// Device-current guard: restores the previous device on scope exit.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (dev != prev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Owning device buffer (move-only).
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  // Allocates exactly `count` elements (frees the previous buffer).
+  int alloc(size_t count) {
+    release();
+    if (count == 0) return ADS_OK;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+    }
+    p = static_cast<T*>(q);
+    n = count;
+    return ADS_OK;
+  }
+  // Grows to at least `count` elements, keeping nothing.
+  int reserve(size_t count) { return count <= n ? ADS_OK : alloc(count); }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------- m/z grid
+// The global 1-ppm grid (src/mz_index/mod.rs:4-25) and a coarse lookup table
+// over the grid's float bit patterns that brackets any lower/upper bound to a
+// handful of grid points.
+constexpr int kLutShift = 6;
+
+struct GridView {
+  const float* grid = nullptr;
+  const uint32_t* lut = nullptr;
+  uint32_t n = 0;       // grid length
+  uint32_t n_lut = 0;   // lut length
+  uint32_t bits0 = 0;   // bit pattern of grid[0]
+  float first = 0.0f;
+  float last = 0.0f;
+};
+
+const std::vector<float>& host_grid();
+int device_grid(int device, GridView* out);
+
+// Gaussian kernel of PeakGroupSelection::new (src/kernel/mod.rs:13-56).
+std::vector<float> gaussian_kernel(float fwhm_rt, float sigma_scale_rt, int64_t kernel_width,
+                                   float rt_resolution);
+
+__device__ __forceinline__ uint32_t f2bits(float x) { return __float_as_uint(x); }
+
+// First i with grid[i] >= x (lower_bound), exact for every float x, NaN -> 0.
+__device__ __forceinline__ uint32_t grid_lower_bound(const GridView& g, float x) {
+  if (!(x > g.first)) return 0;
+  if (x > g.last) return g.n;
+  uint32_t k = (f2bits(x) - g.bits0) >> kLutShift;
+  uint32_t lo = __ldg(g.lut + k), hi = __ldg(g.lut + k + 1);
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(g.grid + mid) < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// First i with grid[i] > x (upper_bound), exact, NaN -> 0.
+__device__ __forceinline__ uint32_t grid_upper_bound(const GridView& g, float x) {
+  if (!(x >= g.first)) return 0;
+  if (!(x < g.last)) return g.n;
+  uint32_t k = (f2bits(x) - g.bits0) >> kLutShift;
+  uint32_t lo = __ldg(g.lut + k), hi = __ldg(g.lut + k + 1);
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(g.grid + mid) <= x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// MZIndex::find_closest_index (src/mz_index/mod.rs:55-90): nearest grid point,
+// ties to the lower index, clamped to the ends.
+__device__ __forceinline__ uint32_t grid_find_closest(const GridView& g, float mz) {
+  uint32_t left = grid_lower_bound(g, mz);
+  if (left == 0) return 0;
+  if (left == g.n) return g.n - 1;
+  float a = __ldg(g.grid + left);
+  if (a == mz) return left;
+  float ld = fabsf(__fsub_rn(a, mz));
+  float rd = fabsf(__fsub_rn(__ldg(g.grid + left - 1), mz));
+  return ld < rd ? left : left - 1;
+}
+
+// ln(x) of a float rounded to the nearest float: evaluated in double and rounded
+// once.  (The reference calls glibc logf, which is not correctly rounded for
+// about 1e-3 of its inputs; see the design notes.)
+__device__ __forceinline__ float ln_rn(float x) { return __double2float_rn(log((double)x)); }
+
+// ------------------------------------------------------------- structures
+struct WinInfo {
+  float lo, hi;      // isolation window, inclusive at both ends
+  int64_t base;      // first entry of this observation in the entry arrays
+  int64_t ss_off;    // element offset of its slice_starts, -1 if it holds no peaks
+};
+
+}  // namespace ads
+
+struct AdsDia {
+  int device = 0;
+  int64_t n_obs = 0;
+  int64_t grid_len = 0;
+  std::vector<ads::WinInfo> win;
+  std::vector<int64_t> num_cycles, num_peaks;
+  ads::DevBuf<ads::WinInfo> win_dev;
+  ads::DevBuf<uint32_t> slice_starts;  // [slots x (grid_len + 1)]
+  ads::DevBuf<uint16_t> cycles;
+  ads::DevBuf<float> intens;
+  ads::DevBuf<uint16_t> intens_bf16;   // built on first BF16 search
+  int64_t n_entries = 0;
+  int max_overlap = 0;                 // max number of non-empty windows covering one m/z
+  std::vector<float> rt;               // MS1 retention times (RT index)
+  float delta_t = 1.0f;
+  ads::DevBuf<float> rt_dev;
+  std::vector<float> rt_values;        // every spectrum's RT (DIAData.rt_values)
+  std::vector<float> cycle;
+  int64_t cycle_shape[4] = {0, 0, 0, 0};
+  std::mutex mu;
+};
+
+struct AdsLib {
+  int device = 0;
+  int64_t n_prec = 0, n_frag = 0;
+  int64_t max_frag = 0;  // max fragments of one precursor
+  ads::DevBuf<uint64_t> pidx;    // sorted precursor_idx
+  ads::DevBuf<float> pmz, prt, ptol;
+  ads::DevBuf<uint64_t> fstart, fstop;
+  ads::DevBuf<float> fmz, fint;
+  ads::DevBuf<uint8_t> fnum, ftype;
+  bool has_tol = false;
+  float max_tol = 0.0f;
+};

@@ -1,0 +1,554 @@
+#!/usr/bin/env python
+"""Benchmark: precursors/s of peak-group selection (XIC + convolution + score +
+top-k + compaction) on B200.
+
+Workload (default ``cfg1``): a synthetic Astral-scale DIA run of 3000 cycles x 300
+MS2 windows of 2 Th (380-980 m/z), 1000 peaks per spectrum (~0.95 G peaks incl.
+planted signal, ~8.5 GB resident), and 200,000 precursors x 12 fragments; search
+settings RT +-150 s, 15 ppm, Gaussian sigma 2 cycles (kernel_size 21), top-3.
+Data are generated on the device from a fixed seed (no dataset is used).
+
+One step = one PeakGroupSelection.search over the whole library with inputs
+resident in HBM.  Inputs are far larger than L2 (126 MB), so no L2 flush is
+needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 the script runs one rank per GPU (torchrun); every rank searches its own
+library of the same size against its own copy of the run (weak scaling, no
+collective on the data path); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RUN_KEYS = ("spectrum_delta_scan_idx", "isolation_lower_mz", "isolation_upper_mz",
+            "spectrum_peak_start_idx", "spectrum_peak_stop_idx", "spectrum_cycle_idx",
+            "spectrum_rt", "peak_mz", "peak_intensity")
+METRIC = "precursors/s (XIC+conv+score+top-k) on 1 B200: batched-BF16 vs plain FP32"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg1")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-windows", type=int, default=24,
+                    help="MS2 windows in the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--warps-per-block", type=int, default=0)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    def __init__(self, device_index: int):
+        self.samples = []
+        self._stop = threading.Event()
+        self._thr = None
+        self.max_mhz = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            h = None
+            for i in range(pynvml.nvmlDeviceGetCount()):
+                hh = pynvml.nvmlDeviceGetHandleByIndex(i)
+                u = pynvml.nvmlDeviceGetUUID(hh)
+                u = u.decode() if isinstance(u, bytes) else u
+                if u.replace("GPU-", "") == uuid.replace("GPU-", ""):
+                    h = hh
+            self.h = h if h is not None else pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: clocks reported as unavailable
+            self.nv = None
+            self.err = str(e)
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((sm, int(reasons)))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def __enter__(self):
+        if self.nv is not None:
+            self._thr = threading.Thread(target=self._run, daemon=True)
+            self._thr.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._thr:
+            self._thr.join()
+
+    def summary(self):
+        if self.nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        nv = self.nv
+        names = {
+            getattr(nv, "nvmlClocksEventReasonGpuIdle", 0x1): "gpu_idle",
+            getattr(nv, "nvmlClocksEventReasonApplicationsClocksSetting", 0x2): "applications_clocks_setting",
+            getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4): "sw_power_cap",
+            getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8): "hw_slowdown",
+            getattr(nv, "nvmlClocksEventReasonSyncBoost", 0x10): "sync_boost",
+            getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20): "sw_thermal_slowdown",
+            getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40): "hw_thermal_slowdown",
+            getattr(nv, "nvmlClocksEventReasonHwPowerBrakeSlowdown", 0x80): "hw_power_brake_slowdown",
+            getattr(nv, "nvmlClocksEventReasonDisplayClockSetting", 0x100): "display_clock_setting",
+        }
+        seen = 0
+        for _, r in self.samples:
+            seen |= r
+        reasons = sorted(n for bit, n in names.items() if seen & bit)
+        med = statistics.median([s for s, _ in self.samples]) if self.samples else None
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------- workload
+
+def make_device_workload(name: str, device: str, lib_seed_offset: int = 0):
+    from alphadia_search_rs_b200 import synth
+
+    cfg = synth.get_config(name)
+    lib_cfg = synth.get_config(name, seed=cfg.seed + 1000 * lib_seed_offset) if lib_seed_offset else cfg
+    lib = synth.make_library(lib_cfg, "torch", device)
+    run = synth.make_run(cfg, lib, "torch", device)
+    return cfg, lib, run
+
+
+def library_tensors(lib: dict, device: str):
+    """SpecLibFlat.from_arrays keyword tensors on the device (reference dtypes)."""
+    import torch
+
+    P = lib["precursor_idx"].numel()
+    NF = lib["fragment_mz"].numel()
+    d = torch.device(device)
+    out = dict(
+        precursor_idx=lib["precursor_idx"].to(torch.uint64),
+        precursor_mz_library=lib["precursor_mz"], precursor_mz=lib["precursor_mz"],
+        precursor_rt_library=lib["precursor_rt"], precursor_rt=lib["precursor_rt"],
+        precursor_naa=torch.full((P,), 10, dtype=torch.uint8, device=d),
+        flat_frag_start_idx=lib["flat_frag_start_idx"].to(torch.uint64),
+        flat_frag_stop_idx=lib["flat_frag_stop_idx"].to(torch.uint64),
+        fragment_mz_library=lib["fragment_mz"], fragment_mz=lib["fragment_mz"],
+        fragment_intensity=lib["fragment_intensity"],
+        fragment_cardinality=torch.ones(NF, dtype=torch.uint8, device=d),
+        fragment_charge=torch.ones(NF, dtype=torch.uint8, device=d),
+        fragment_loss_type=torch.zeros(NF, dtype=torch.uint8, device=d),
+        fragment_number=lib["fragment_number"].to(torch.uint8),
+        fragment_position=torch.ones(NF, dtype=torch.uint8, device=d),
+        fragment_type=lib["fragment_type"].to(torch.uint8),
+    )
+    out = {k: v.contiguous() for k, v in out.items()}
+    if lib.get("rt_tolerance") is not None:
+        out["precursor_rt_tolerance"] = lib["rt_tolerance"].contiguous()
+    return out
+
+
+def window_subset(cfg, run: dict, lib: dict, n_windows: int):
+    """Host copy of the MS1 spectra plus ``n_windows`` consecutive MS2 windows from
+    the middle of the run, and the library precursors whose every valid window lies
+    in that subset (strictly inside its m/z span).  Windows are renumbered 1..n."""
+    import torch
+
+    W = cfg.n_windows
+    w0 = max(1, (W - n_windows) // 2 + 1)
+    w1 = min(W, w0 + n_windows - 1)
+    dsi = run["spectrum_delta_scan_idx"]
+    keep = (dsi == 0) | ((dsi >= w0) & (dsi <= w1))
+    sidx = torch.nonzero(keep).flatten()
+    st, sp = run["spectrum_peak_start_idx"], run["spectrum_peak_stop_idx"]
+    counts = (sp - st)[sidx]
+    # peaks of the kept spectra, in spectrum order
+    owner = torch.repeat_interleave(torch.arange(sidx.numel(), device=dsi.device), counts)
+    first = torch.cumsum(counts, 0) - counts
+    pk = st[sidx][owner] + (torch.arange(owner.numel(), device=dsi.device) - first[owner])
+    new_stop = torch.cumsum(counts, 0)
+    new_start = new_stop - counts
+    new_dsi = dsi[sidx].clone()
+    new_dsi[new_dsi > 0] -= (w0 - 1)
+    host = dict(
+        spectrum_delta_scan_idx=new_dsi.cpu().numpy().astype(np.int64),
+        isolation_lower_mz=run["isolation_lower_mz"][sidx].cpu().numpy(),
+        isolation_upper_mz=run["isolation_upper_mz"][sidx].cpu().numpy(),
+        spectrum_peak_start_idx=new_start.cpu().numpy().astype(np.int64),
+        spectrum_peak_stop_idx=new_stop.cpu().numpy().astype(np.int64),
+        spectrum_cycle_idx=run["spectrum_cycle_idx"][sidx].cpu().numpy().astype(np.int64),
+        spectrum_rt=run["spectrum_rt"][sidx].cpu().numpy(),
+        peak_mz=run["peak_mz"][pk].cpu().numpy(),
+        peak_intensity=run["peak_intensity"][pk].cpu().numpy(),
+        cycle=np.zeros((n_windows + 1, 1, 1, 1), np.float32),
+    )
+    lo = np.float32(cfg.window_start + (w0 - 1) * cfg.window_width)
+    hi = np.float32(cfg.window_start + w1 * cfg.window_width)
+    pmz = lib["precursor_mz"].cpu().numpy()
+    sel = np.nonzero((pmz > lo) & (pmz < hi))[0]
+    fs = lib["flat_frag_start_idx"].cpu().numpy()
+    fe = lib["flat_frag_stop_idx"].cpu().numpy()
+    nf = fe[sel] - fs[sel]
+    fidx = np.concatenate([np.arange(a, b) for a, b in zip(fs[sel], fe[sel])]) if len(sel) else np.zeros(0, np.int64)
+    new_fe = np.cumsum(nf)
+    sub = dict(
+        precursor_idx=lib["precursor_idx"].cpu().numpy()[sel].astype(np.uint64),
+        precursor_mz=pmz[sel], precursor_rt=lib["precursor_rt"].cpu().numpy()[sel],
+        flat_frag_start_idx=(new_fe - nf).astype(np.uint64), flat_frag_stop_idx=new_fe.astype(np.uint64),
+        fragment_mz=lib["fragment_mz"].cpu().numpy()[fidx],
+        fragment_intensity=lib["fragment_intensity"].cpu().numpy()[fidx],
+        fragment_number=lib["fragment_number"].cpu().numpy()[fidx].astype(np.uint8),
+        fragment_type=lib["fragment_type"].cpu().numpy()[fidx].astype(np.uint8),
+    )
+    if lib.get("rt_tolerance") is not None:
+        sub["rt_tolerance"] = lib["rt_tolerance"].cpu().numpy()[sel]
+    return host, sub, (w0, w1)
+
+
+def oracle_setup(host: dict, sub: dict, n_threads: int):
+    import oracle
+
+    od = oracle.Dia(**{k: host[k] for k in RUN_KEYS}, n_threads=n_threads)
+    ol = oracle.Lib(sub["precursor_idx"], sub["precursor_mz"], sub["precursor_rt"],
+                    sub["flat_frag_start_idx"], sub["flat_frag_stop_idx"], sub["fragment_mz"],
+                    sub["fragment_intensity"], sub["fragment_number"], sub["fragment_type"])
+    tol = None
+    if "rt_tolerance" in sub:
+        tol = np.asarray(sub["rt_tolerance"], np.float32)[ol.sorted_order]
+    return od, ol, tol
+
+
+def time_oracle(od, ol, tol, params, n_threads, steps, warmup):
+    import oracle
+
+    p = oracle.Params(**params)
+    res = None
+    for _ in range(warmup):
+        res = oracle.search(od, ol, p, rt_tolerance_per_precursor=tol, n_threads=n_threads)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        res = oracle.search(od, ol, p, rt_tolerance_per_precursor=tol, n_threads=n_threads)
+        ts.append(time.perf_counter() - t0)
+    return ts, res
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def load_traffic(name: str):
+    """Per-launch DRAM bytes of the search kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"search_kernel_{name}.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------- reference arm
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import torch
+
+    from alphadia_search_rs_b200 import synth
+
+    device = "cuda:0"
+    cfg, lib, run = make_device_workload(args.workload, device)
+    host, sub, (w0, w1) = window_subset(cfg, run, lib, args.cpu_windows)
+    del run
+    torch.cuda.empty_cache()
+    n = cpu_threads()
+    od, ol, tol = oracle_setup(host, sub, n)
+    ts, res = time_oracle(od, ol, tol, cfg.params_dict(), n, args.steps, args.warmup)
+    P = len(sub["precursor_idx"])
+    mean = statistics.mean(ts)
+    value = P / mean
+    sample = (f"{P} precursors of the {cfg.n_precursors} whose m/z lies inside MS2 windows "
+              f"{w0}-{w1} ({w1 - w0 + 1} of {cfg.n_windows}), searched against those windows' "
+              f"{len(host['peak_mz'])} peaks")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "precursors/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded, generated on the device)",
+        "config": {"workload": f"{cfg.name}: {cfg.n_cycles} cycles x {cfg.n_windows} windows, "
+                               f"{cfg.n_precursors} precursors", "sample_windows": [w0, w1]},
+        "cpu_baseline": {"value": value, "unit": "precursors/s", "cores": n, "kind": "port",
+                         "sample": sample, "cpu_model": cpu_model()},
+        "e2e": {"value": value, "unit": "precursors/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "candidates_per_step": int(len(res["rank"])),
+        "reference_note": "the reference crate is Rust and cannot be built here (no cargo); its scalar "
+                          "path is timed as the C++ restatement in oracle/ with all host threads",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import alphadia_search_rs_b200 as ads
+
+    device = f"cuda:{local_rank}"
+    torch.cuda.set_device(local_rank)
+    t_setup = time.perf_counter()
+    cfg, lib, run = make_device_workload(args.workload, device, lib_seed_offset=rank)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_setup
+    t0 = time.perf_counter()
+    dia = ads.DIAData.from_arrays(*(run[k] for k in RUN_KEYS), run["cycle"], device=local_rank)
+    t_dia = time.perf_counter() - t0
+    ltens = library_tensors(lib, device)
+    t0 = time.perf_counter()
+    slib = ads.SpecLibFlat.from_arrays(**ltens, device=local_rank)
+    t_lib = time.perf_counter() - t0
+    P = slib.num_precursors
+    params = ads.SelectionParameters()
+    params.update(cfg.params_dict())
+
+    # counters pass (untimed): algorithmic bytes of the gather
+    sel_stats = ads.PeakGroupSelection(params, verbose=False, device=local_rank)
+    sel_stats.enable_stats(True)
+    cand_full = sel_stats.search(dia, slib)
+    stats = sel_stats.last_stats()
+    n_cand = cand_full.len()
+    full_arrays = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        full_arrays = cand_full.to_arrays()
+    del cand_full, sel_stats
+
+    sel = ads.PeakGroupSelection(params, verbose=False, device=local_rank, time_stages=True,
+                                 warps_per_block=args.warps_per_block,
+                                 blocks_per_sm=args.blocks_per_sm)
+    cand = sel.new_candidates()
+    stream = torch.cuda.ExternalStream(sel.stream, device=device)
+    for _ in range(args.warmup):
+        sel.search_into(dia, slib, cand)
+    cand.size()
+    sel.stage_times()  # discard warm-up stage timings
+    launches_per_step = sel.last_launches
+
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        td.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            sel.search_into(dia, slib, cand)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        td.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if cand.size() != n_cand:
+        raise RuntimeError("candidate count changed between searches")
+    st = sel.stage_times()
+    ms_t = torch.tensor([ms], device=device, dtype=torch.float64)
+    if dist:
+        td.all_reduce(ms_t, op=td.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = P * world * args.steps / (ms_max / 1e3)
+
+    # ---- end to end through the public API with pinned host buffers
+    lib_host = {k: v.cpu().pin_memory() for k, v in ltens.items()}
+    lib_np = {k: v.numpy() for k, v in lib_host.items()}
+    cap = max(n_cand, 1)
+    out_t = [torch.empty(cap, dtype=torch.float32 if i == 2 else torch.uint64).pin_memory() for i in range(9)]
+    out_np = tuple(t.numpy() for t in out_t)
+    sel_e2e = ads.PeakGroupSelection(params, verbose=False, device=local_rank)
+    h2d = sum(lib_np[k].nbytes for k in ("precursor_idx", "precursor_mz", "precursor_rt",
+                                          "flat_frag_start_idx", "flat_frag_stop_idx", "fragment_mz",
+                                          "fragment_intensity", "fragment_number", "fragment_type"))
+    if "precursor_rt_tolerance" in lib_np:
+        h2d += lib_np["precursor_rt_tolerance"].nbytes
+    e2e_times = []
+    d2h = 0
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        l2 = ads.SpecLibFlat.from_arrays(**lib_np, device=local_rank)
+        c2 = sel_e2e.search(dia, l2)
+        arrs = c2.to_arrays(out=out_np)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        d2h = len(arrs[0]) * (5 * 8 + 4)
+        del l2, c2
+        if i > 0:  # first call warms up allocations
+            e2e_times.append(dt)
+    e2e_t = torch.tensor([statistics.mean(e2e_times)], device=device, dtype=torch.float64)
+    if dist:
+        td.all_reduce(e2e_t, op=td.ReduceOp.MAX)
+    e2e_value = P * world / float(e2e_t.item())
+
+    if rank != 0:
+        return
+
+    # ---- roofline of the dominant kernel (search_kernel)
+    n_searches = max(st["searches"], 1)
+    search_ms = st["search_ms"] / n_searches
+    prep_ms = st["prep_ms"] / n_searches
+    comp_ms = st["compaction_ms"] / n_searches
+    s_i = 4  # f32 intensities
+    gather_bytes = 4 * stats["bins_plus_one"] + (2 + s_i) * stats["entries_accumulated"]
+    nf_raw = int(lib["fragment_mz"].numel())
+    path_bytes = 8 * P + 8 * nf_raw + gather_bytes + 68 * n_cand
+    peak, peak_kind = measured_peak()
+    achieved = gather_bytes / (search_ms / 1e3) / 1e9
+    traffic = load_traffic(cfg.name)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel": "search_kernel",
+                "algorithmic_bytes_per_launch": gather_bytes,
+                "kernel_ms_per_launch": search_ms,
+                "path_bytes_per_step": path_bytes,
+                "path_gbs": path_bytes / (ms_max / args.steps / 1e3) / 1e9,
+                "stage_ms": {"prep": prep_ms, "search": search_ms, "compaction": comp_ms}}
+
+    # ---- CPU baseline (oracle port on the host cores, bounded sample) and a
+    #      parity spot check of the GPU result for the same precursors
+    cpu = None
+    parity = None
+    if world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        host, sub, (w0, w1) = window_subset(cfg, run, lib, args.cpu_windows)
+        n = cpu_threads()
+        od, ol, tol = oracle_setup(host, sub, n)
+        ts, res = time_oracle(od, ol, tol, cfg.params_dict(), n, steps=3, warmup=1)
+        Ps = len(sub["precursor_idx"])
+        cpu = {"value": Ps / statistics.mean(ts), "unit": "precursors/s", "cores": n, "kind": "port",
+               "sample": f"{Ps} precursors inside MS2 windows {w0}-{w1} ({w1 - w0 + 1} of "
+                         f"{cfg.n_windows}) against those windows' {len(host['peak_mz'])} peaks; "
+                         f"mean of 3 timed searches",
+               "cpu_model": cpu_model()}
+        got = dict(zip(("precursor_idx", "rank", "score", "sc", "ss", "sp", "cycle_center",
+                        "cycle_start", "cycle_stop"), full_arrays))
+        mask = np.isin(got["precursor_idx"], sub["precursor_idx"])
+        same = {k: bool(np.array_equal(got[k][mask], res[k])) for k in
+                ("precursor_idx", "rank", "cycle_center", "cycle_start", "cycle_stop")}
+        rel = 0.0
+        if mask.sum() == len(res["score"]) and len(res["score"]):
+            rel = float(np.max(np.abs(got["score"][mask].astype(np.float64) - res["score"]) /
+                               np.maximum(np.abs(res["score"]).astype(np.float64), 1e-30)))
+        parity = {"precursors": int(len(sub["precursor_idx"])), "candidates": int(len(res["rank"])),
+                  "indices_identical": all(same.values()) and int(mask.sum()) == len(res["rank"]),
+                  "max_score_rel_err_vs_glibc_logf": rel}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "precursors/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded, generated on the device)",
+        "config": {"workload": f"{cfg.name}: {cfg.n_cycles} cycles x {cfg.n_windows} MS2 windows of "
+                               f"{cfg.window_width} Th, {cfg.peaks_per_spectrum} peaks/spectrum, "
+                               f"{cfg.n_precursors} precursors x {cfg.frag_min}-{cfg.frag_max} fragments",
+                   "precision": "fp32", "params": cfg.params_dict(),
+                   "l2": "inputs larger than L2 (resident run ~%.1f GB), no flush" %
+                         (dia.memory_footprint_bytes() / 1e9),
+                   "peaks": int(run["peak_mz"].numel()), "candidates_per_step": int(n_cand),
+                   "precursors_per_gpu": int(P), "parallelism": f"replicated run, {world} library shard(s)"},
+        "e2e": {"value": e2e_value, "unit": "precursors/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h),
+                "path": "SpecLibFlat.from_arrays(pinned host arrays) + PeakGroupSelection.search + "
+                        "CandidateCollection.to_arrays(out=pinned)"},
+        "gpu_launches": int(launches_per_step * args.steps),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "parity_sample": parity,
+        "clocks": clk.summary(),
+        "setup_s": {"generate": t_gen, "dia_build": t_dia, "lib_build": t_lib},
+        "counters": stats,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and world > 1:
+        print(f"WORLD_SIZE={world} but --gpus {args.gpus}", file=sys.stderr)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+
+        torch.cuda.set_device(local_rank)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                              device_id=torch.device(f"cuda:{local_rank}"))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as td
+
+            td.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,230 @@
+/*
+ * ads_gpu.h — C ABI of the B200-native peak-group-selection engine.
+ *
+ * Drop-in boundary for `PeakGroupSelection.search` of MannLabs/alphadia-search-rs.
+ * Each entry point names the reference interface it replaces (file:line in the
+ * reference crate).  The ABI is plain C: opaque handles, plain pointers and sizes,
+ * int status codes.  Nothing here throws or aborts across the boundary.
+ *
+ * Ownership: input arrays are borrowed for the duration of a call only (the
+ * reference copies its numpy inputs too).  Handles own their device buffers and are
+ * released by the matching *_destroy.  Candidate arrays are copied into
+ * caller-allocated memory by ads_candidates_copy_out.
+ *
+ * Threading: calls on different handles may run concurrently.  A selection handle
+ * owns one CUDA stream; calls that share a selection handle must be serialised by
+ * the caller.  Error text is kept per host thread (ads_last_error).
+ */
+#ifndef ADS_GPU_H
+#define ADS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define ADS_OK 0
+#define ADS_ERR_INVALID_ARGUMENT 1 /* Python: ValueError */
+#define ADS_ERR_OUT_OF_MEMORY 2    /* Python: MemoryError */
+#define ADS_ERR_CUDA 3             /* Python: RuntimeError */
+#define ADS_ERR_DEVICE_TIMEOUT 4   /* a bounded device-side wait ran out */
+#define ADS_ERR_INTERNAL 5
+
+#define ADS_MEM_HOST 0   /* array pointers are host memory */
+#define ADS_MEM_DEVICE 1 /* array pointers are device memory of the handle's device */
+
+#define ADS_PRECISION_FP32 0 /* f32 intensities, XIC and convolution (reference numerics) */
+#define ADS_PRECISION_BF16 1 /* bf16-stored intensities; f32 accumulation, log and score */
+
+/* Error text of the last failing call on this host thread ("" if none). */
+const char* ads_last_error(void);
+/* Library version string. */
+const char* ads_version(void);
+/* Number of CUDA devices visible (0 when there is none); never fails. */
+int ads_device_count(void);
+
+/* ------------------------------------------------------------------ DIAData
+ * Replaces DIAData::from_arrays (src/dia_data/mod.rs:43-72), which builds through
+ * DIADataBuilder::from_alpha_raw (src/dia_data_builder/mod.rs:11-139).  Argument
+ * meaning follows the reference's numpy arrays; `cycle` is the 4-D float array the
+ * reference stores and returns unchanged (may be NULL with all dims 0).
+ */
+typedef struct AdsDia AdsDia;
+
+typedef struct {
+  int32_t location; /* ADS_MEM_HOST or ADS_MEM_DEVICE for the spectrum and peak arrays */
+  int64_t n_spectra;
+  const int64_t* spectrum_delta_scan_idx;
+  const float* isolation_lower_mz;
+  const float* isolation_upper_mz;
+  const int64_t* spectrum_peak_start_idx;
+  const int64_t* spectrum_peak_stop_idx;
+  const int64_t* spectrum_cycle_idx;
+  const float* spectrum_rt;
+  int64_t n_peaks;
+  const float* peak_mz;
+  const float* peak_intensity;
+  const float* cycle; /* host memory always */
+  int64_t cycle_shape[4];
+} AdsRawArrays;
+
+int ads_dia_create(const AdsRawArrays* raw, int device, AdsDia** out);
+int ads_dia_destroy(AdsDia* dia);
+/* DIAData.num_observations (src/dia_data/mod.rs:74-77) */
+int64_t ads_dia_num_observations(const AdsDia* dia);
+/* DIAData.memory_footprint_bytes (src/dia_data/mod.rs:90-105): same accounting
+ * (rt index + per-observation slice_starts/cycle_indices/intensities + fixed parts). */
+int64_t ads_dia_memory_footprint_bytes(const AdsDia* dia);
+/* DIAData.rt_values / cycle getters (src/dia_data/mod.rs:127-135).  Copies into host
+ * memory; returns the element count in *n (pass out = NULL to query). */
+int ads_dia_rt_values(const AdsDia* dia, float* out, int64_t cap, int64_t* n);
+int ads_dia_cycle(const AdsDia* dia, float* out, int64_t cap, int64_t shape[4]);
+/* RT index of MS1 scans (src/rt_index/mod.rs:53-75). */
+int ads_dia_rt_index(const AdsDia* dia, float* out, int64_t cap, int64_t* n, float* delta_t);
+/* One quadrupole observation (src/quadrupole_observation/mod.rs:12-25):
+ * isolation window, number of unique cycles, number of peaks. */
+int ads_dia_observation_info(const AdsDia* dia, int64_t obs, float* iso_lower, float* iso_upper,
+                             int64_t* num_cycles, int64_t* num_peaks);
+/* Copies one observation's CSR to host: slice_starts (grid_len + 1 entries),
+ * cycle_indices and intensities (num_peaks entries each).  Any pointer may be NULL. */
+int ads_dia_copy_observation(const AdsDia* dia, int64_t obs, uint32_t* slice_starts,
+                             uint16_t* cycle_indices, float* intensities);
+/* Length of the global 1-ppm m/z grid (src/mz_index/mod.rs:4-6,27). */
+int64_t ads_mz_grid_len(void);
+int ads_mz_grid(float* out, int64_t cap);
+
+/* ---------------------------------------------------------------- SpecLibFlat
+ * Replaces SpecLibFlat::from_arrays (src/speclib_flat/mod.rs:100-188): precursor
+ * arrays are stably sorted by precursor_idx, fragment arrays keep their order.
+ * Arrays the selection path never reads (library m/z and RT, nAA, cardinality,
+ * charge, loss type, position) may be NULL.  precursor_rt_tolerance is an
+ * extension: an optional per-precursor RT half-window in seconds that replaces
+ * SelectionParameters.rt_tolerance for that precursor (NULL = the global value).
+ */
+typedef struct AdsLib AdsLib;
+
+typedef struct {
+  int32_t location; /* ADS_MEM_HOST or ADS_MEM_DEVICE */
+  int64_t n_precursors;
+  const uint64_t* precursor_idx;
+  const float* precursor_mz_library;
+  const float* precursor_mz;
+  const float* precursor_rt_library;
+  const float* precursor_rt;
+  const uint8_t* precursor_naa;
+  const uint64_t* flat_frag_start_idx;
+  const uint64_t* flat_frag_stop_idx;
+  int64_t n_fragments;
+  const float* fragment_mz_library;
+  const float* fragment_mz;
+  const float* fragment_intensity;
+  const uint8_t* fragment_cardinality;
+  const uint8_t* fragment_charge;
+  const uint8_t* fragment_loss_type;
+  const uint8_t* fragment_number;
+  const uint8_t* fragment_position;
+  const uint8_t* fragment_type;
+  const float* precursor_rt_tolerance; /* extension, may be NULL */
+} AdsLibArrays;
+
+int ads_lib_create(const AdsLibArrays* arrays, int device, AdsLib** out);
+int ads_lib_destroy(AdsLib* lib);
+/* SpecLibFlat.num_precursors / num_fragments (src/speclib_flat/mod.rs:190-198) */
+int64_t ads_lib_num_precursors(const AdsLib* lib);
+int64_t ads_lib_num_fragments(const AdsLib* lib);
+
+/* ------------------------------------------------------- PeakGroupSelection
+ * SelectionParameters (src/peak_group_selection/parameters.rs:4-43): same seven
+ * fields, same meaning, same defaults (ads_selection_params_default).
+ */
+typedef struct {
+  float fwhm_rt;
+  int64_t kernel_size;
+  int64_t peak_length;
+  float mass_tolerance;
+  float rt_tolerance;
+  int64_t candidate_count;
+  int64_t top_k_fragments;
+} AdsSelectionParams;
+
+/* Engine options beyond the reference's parameters. */
+typedef struct {
+  int32_t precision;   /* ADS_PRECISION_FP32 (default) or ADS_PRECISION_BF16 */
+  int32_t verbose;     /* 1: print the reference's two lines after each search
+                          (src/peak_group_selection/mod.rs:123-125) */
+  int32_t use_graph;   /* 1: capture the search pipeline in a CUDA graph and replay it */
+  int32_t warps_per_block; /* 0 = autotuned/default */
+  int32_t blocks_per_sm;   /* 0 = autotuned/default */
+  int32_t gather_mode;     /* 0 = automatic, 1 = always scan bin ranges, 2 = always
+                              binary-search each bin (both are exact; for testing) */
+  int32_t time_stages;     /* 1: record CUDA events around each stage of a search */
+  int64_t stream;          /* cudaStream_t to run on, 0 = the handle's own stream */
+} AdsEngineOptions;
+
+void ads_selection_params_default(AdsSelectionParams* p);
+void ads_engine_options_default(AdsEngineOptions* o);
+
+/* GaussianKernel::new(fwhm_rt, sigma_scale_rt, kernel_width, rt_resolution)
+ * (src/kernel/mod.rs:13-56) on the host: writes the weights and their count (the
+ * width rounded up to even).  Needs no device. */
+int ads_gaussian_kernel(float fwhm_rt, float sigma_scale_rt, int64_t kernel_width,
+                        float rt_resolution, float* out, int64_t cap, int64_t* n);
+
+typedef struct AdsSelection AdsSelection;
+typedef struct AdsCandidates AdsCandidates;
+
+/* PeakGroupSelection::new (src/peak_group_selection/mod.rs:74-85): validates the
+ * parameters and builds the Gaussian kernel (src/kernel/mod.rs:13-56) once. */
+int ads_selection_create(const AdsSelectionParams* params, const AdsEngineOptions* options,
+                         int device, AdsSelection** out);
+int ads_selection_destroy(AdsSelection* sel);
+/* Kernel weights the selection uses (length returned in *n). */
+int ads_selection_kernel(const AdsSelection* sel, float* out, int64_t cap, int64_t* n);
+
+/* PeakGroupSelection.search (src/peak_group_selection/mod.rs:87-128): returns a
+ * new candidate collection in the reference's order (library order of
+ * precursor_idx, then rank).  Blocks until the search is done. */
+int ads_select(AdsSelection* sel, const AdsDia* dia, const AdsLib* lib, AdsCandidates** out);
+
+/* Same search, enqueued on the selection's stream without waiting, into an existing
+ * collection whose device buffers are reused (grown if needed).  The collection's
+ * size is read (and the stream synchronised) by ads_candidates_size. */
+int ads_select_async(AdsSelection* sel, const AdsDia* dia, const AdsLib* lib,
+                     AdsCandidates* reuse);
+/* Empty collection bound to a selection's device, for ads_select_async. */
+int ads_candidates_create(const AdsSelection* sel, AdsCandidates** out);
+/* cudaStream_t (as integer) that a selection enqueues its work on. */
+int64_t ads_selection_stream(const AdsSelection* sel);
+/* Number of kernels the last search launched (for launch accounting). */
+int64_t ads_selection_last_launches(const AdsSelection* sel);
+/* Per-search counters of the last search: [0] (fragment, window) pairs gathered,
+ * [1] sum over those pairs of (m/z bins + 1), [2] fragments searched, [3] XIC peak
+ * entries read, [4] XIC peak entries accumulated (n_in), [5] CSR offsets read.
+ * Collected only while enabled with ads_selection_set_stats. */
+int ads_selection_set_stats(AdsSelection* sel, int enabled);
+int ads_selection_last_stats(AdsSelection* sel, int64_t* out, int64_t cap);
+/* Device time in ms of the stages of every search since the previous call, measured
+ * with CUDA events on the selection's stream when created with time_stages = 1:
+ * [0] prep kernel, [1] search kernel, [2] compaction kernels (sums), [3] number of
+ * searches.  Waits for the last recorded search. */
+int ads_selection_stage_times(AdsSelection* sel, float* ms, int64_t cap);
+
+/* ------------------------------------------------------- CandidateCollection
+ * CandidateCollection.len / to_arrays (src/candidate/entry.rs:61-173). */
+int64_t ads_candidates_size(AdsCandidates* cand);
+/* Copies into caller arrays of ads_candidates_size() elements, in the tuple order of
+ * to_arrays: precursor_idx, rank, score, scan_center, scan_start, scan_stop,
+ * cycle_center, cycle_start, cycle_stop (u64 except score f32).  Any pointer may be
+ * NULL to skip that array (the scan_* arrays are always zero, as in the reference). */
+int ads_candidates_copy_out(AdsCandidates* cand, uint64_t* precursor_idx, uint64_t* rank,
+                            float* score, uint64_t* scan_center, uint64_t* scan_start,
+                            uint64_t* scan_stop, uint64_t* cycle_center, uint64_t* cycle_start,
+                            uint64_t* cycle_stop);
+int ads_candidates_destroy(AdsCandidates* cand);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ADS_GPU_H */

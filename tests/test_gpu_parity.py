@@ -1,0 +1,148 @@
+"""GPU parity: the CUDA search (through the C ABI) against the CPU oracle.
+
+Two comparisons per workload:
+  * oracle with a correctly rounded logf (what the kernel computes): every column
+    identical, scores bit for bit -- this pins the kernel's summation order;
+  * oracle with glibc logf (the reference's numerics on Linux): every index
+    column identical, scores within SCORE_RTOL (1e-5) relative.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from alphadia_search_rs_b200 import synth
+
+from _util import (RUN_KEYS, assert_candidates_equal, edge_case_workload, oracle_inputs,
+                   oracle_search, product_search)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", params=["tiny", "tiny_uneven", "cfg0"])
+def workload(request):
+    cfg, lib, run = synth.make_workload(request.param, "numpy")
+    la = synth.library_arrays(lib)
+    od, ol, tol = oracle_inputs(run, la)
+    return cfg, run, la, (od, ol, tol)
+
+
+def test_dia_csr_matches_builder(workload):
+    """DIAData built on the device is word-identical to the restated builder
+    (src/dia_data_builder/mod.rs:52-139)."""
+    cfg, run, la, (od, ol, tol) = workload
+    from alphadia_search_rs_b200 import DIAData
+
+    dia = DIAData.from_arrays(*(run[k] for k in RUN_KEYS), run["cycle"])
+    assert dia.num_observations == od.num_observations
+    rt, dt = dia.rt_index()
+    assert np.array_equal(rt, od.rt) and np.float32(dt) == np.float32(od.delta_t)
+    for w in range(od.num_observations):
+        o = dia.observation(w)
+        assert o["isolation_window"] == od.window(w)
+        assert np.array_equal(o["slice_starts"], od.slice_starts(w)), w
+        assert np.array_equal(o["cycle_indices"], od.cycles(w)), w
+        assert np.array_equal(o["intensities"].view(np.uint32), od.intensities(w).view(np.uint32)), w
+
+
+@pytest.mark.parametrize("gather_mode", [0, 1, 2])
+def test_search_bit_exact_vs_rn_oracle(workload, gather_mode):
+    cfg, run, la, (od, ol, tol) = workload
+    got, *_ = product_search(run, la, cfg.params_dict(), gather_mode=gather_mode)
+    ref = oracle_search(run, la, cfg.params_dict(), oracle.LOG_RN, od, ol, tol)
+    assert len(ref["rank"]) > 0
+    assert_candidates_equal(got, ref, exact_scores=True, where=f"{cfg.name}/mode{gather_mode}")
+
+
+def test_search_vs_reference_numerics(workload):
+    cfg, run, la, (od, ol, tol) = workload
+    got, *_ = product_search(run, la, cfg.params_dict())
+    ref = oracle_search(run, la, cfg.params_dict(), oracle.LOG_GLIBC, od, ol, tol)
+    assert_candidates_equal(got, ref, exact_scores=False, where=cfg.name)
+
+
+def test_search_deterministic(workload):
+    cfg, run, la, _ = workload
+    a, *_ = product_search(run, la, cfg.params_dict())
+    b, *_ = product_search(run, la, cfg.params_dict(), warps_per_block=2)
+    for k in a:
+        assert np.array_equal(np.asarray(a[k]).view(np.uint8), np.asarray(b[k]).view(np.uint8)), k
+
+
+@pytest.mark.parametrize("variant", [
+    dict(),
+    dict(peak_length=15),              # center - peak_length wraps as usize
+    dict(kernel_size=9, fwhm_rt=2.0),
+    dict(kernel_size=62),              # largest supported kernel
+    dict(candidate_count=0),
+    dict(candidate_count=50),
+    dict(top_k_fragments=0),
+    dict(top_k_fragments=3),
+    dict(mass_tolerance=200.0),        # wide bin ranges (binary-search gather)
+    dict(rt_tolerance=5.0),            # minimum tolerance (10 + kernel_size) * delta_t applies
+    dict(rt_tolerance=1000.0),
+])
+def test_edge_cases(variant):
+    run, la = edge_case_workload()
+    params = dict(fwhm_rt=3.0, kernel_size=20, peak_length=5, mass_tolerance=20.0,
+                  rt_tolerance=30.0, candidate_count=3, top_k_fragments=6)
+    params.update(variant)
+    got, *_ = product_search(run, la, params)
+    ref = oracle_search(run, la, params, oracle.LOG_RN)
+    assert_candidates_equal(got, ref, exact_scores=True, where=str(variant))
+    ref_g = oracle_search(run, la, params, oracle.LOG_GLIBC)
+    assert_candidates_equal(got, ref_g, exact_scores=False, where=str(variant))
+
+
+def test_edge_case_csr():
+    run, la = edge_case_workload()
+    from alphadia_search_rs_b200 import DIAData
+
+    od, _, _ = oracle_inputs(run, la)
+    dia = DIAData.from_arrays(*(run[k] for k in RUN_KEYS), run["cycle"])
+    assert dia.num_observations == od.num_observations == 5
+    for w in range(5):
+        o = dia.observation(w)
+        assert np.array_equal(o["slice_starts"], od.slice_starts(w))
+        assert np.array_equal(o["cycle_indices"], od.cycles(w))
+    assert dia.get_valid_observations(425.0) == od.valid_observations(425.0) == [1, 2]
+
+
+def test_empty_library():
+    run, la = edge_case_workload()
+    la = {k: v[:0] for k, v in la.items()}
+    got, *_ = product_search(run, la, dict(candidate_count=3))
+    assert all(len(v) == 0 for v in got.values())
+
+
+def test_device_inputs_match_host_inputs():
+    import torch
+
+    from alphadia_search_rs_b200 import DIAData, PeakGroupSelection, SpecLibFlat
+
+    from _util import params_from
+
+    cfg, lib, run = synth.make_workload("tiny", "numpy")
+    la = synth.library_arrays(lib)
+    host, *_ = product_search(run, la, cfg.params_dict())
+    dev = {k: torch.from_numpy(np.ascontiguousarray(run[k])).cuda() for k in RUN_KEYS}
+    dia = DIAData.from_arrays(*(dev[k] for k in RUN_KEYS), run["cycle"])
+    ldev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in la.items()}
+    sl = SpecLibFlat.from_arrays(**ldev)
+    cand = PeakGroupSelection(params_from(cfg.params_dict()), verbose=False).search(dia, sl)
+    arrs = cand.to_arrays()
+    for k, a in zip(host, arrs):
+        assert np.array_equal(np.asarray(host[k]).view(np.uint8), a.view(np.uint8)), k
+
+
+def test_verbose_prints_reference_lines(capfd):
+    from alphadia_search_rs_b200 import PeakGroupSelection
+
+    from _util import params_from
+
+    cfg, lib, run = synth.make_workload("tiny", "numpy")
+    la = synth.library_arrays(lib)
+    _, dia, sl, _ = product_search(run, la, cfg.params_dict())
+    cand = PeakGroupSelection(params_from(cfg.params_dict())).search(dia, sl)
+    out = capfd.readouterr().out
+    assert "Precursors per second:" in out
+    assert f"Found {cand.len()} candidates" in out
