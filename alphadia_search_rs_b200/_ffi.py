@@ -6,6 +6,7 @@ library is missing: there is no CPU fallback.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
 
@@ -138,6 +139,22 @@ SIGNATURES = {
 }
 
 _lib = None
+_finalizing = False
+
+
+def _mark_finalizing():
+    global _finalizing
+    _finalizing = True
+
+
+atexit.register(_mark_finalizing)
+
+
+def alive() -> bool:
+    """False once the interpreter is shutting down: handles are then left to the
+    process exit instead of being destroyed through a runtime that may already be
+    torn down."""
+    return _lib is not None and not _finalizing
 
 
 class AdsError(RuntimeError):

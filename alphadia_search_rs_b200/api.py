@@ -65,7 +65,7 @@ class DIAData:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and F.alive():
             try:
                 _lib().ads_dia_destroy(h)
             except Exception:
@@ -221,7 +221,7 @@ class SpecLibFlat:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and F.alive():
             try:
                 _lib().ads_lib_destroy(h)
             except Exception:
@@ -369,7 +369,7 @@ class CandidateCollection:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and F.alive():
             try:
                 _lib().ads_candidates_destroy(h)
             except Exception:
@@ -476,7 +476,7 @@ class PeakGroupSelection:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and F.alive():
             try:
                 _lib().ads_selection_destroy(h)
             except Exception:
@@ -544,7 +544,7 @@ class DeviceCandidates:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and F.alive():
             try:
                 _lib().ads_candidates_destroy(h)
             except Exception:

@@ -22,6 +22,7 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
   snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e),
            what, file, line);
   g_last_error = buf;
+  cudaGetLastError();  // a non-sticky error must not resurface in a later, unrelated call
   return e == cudaErrorMemoryAllocation ? ADS_ERR_OUT_OF_MEMORY : ADS_ERR_CUDA;
 }
 
@@ -102,6 +103,33 @@ int device_grid(int device, GridView* out) {
   st.view.last = g[n - 1];
   g_grids[device] = st;
   *out = st.view;
+  return ADS_OK;
+}
+
+namespace {
+std::mutex g_ln_mu;
+std::map<int, double2*> g_ln_tables;
+}  // namespace
+
+int device_ln_table(int device, const double2** out) {
+  std::lock_guard<std::mutex> lk(g_ln_mu);
+  auto it = g_ln_tables.find(device);
+  if (it != g_ln_tables.end()) {
+    *out = it->second;
+    return ADS_OK;
+  }
+  std::vector<double2> tab(kLnTableSize);
+  for (int j = 0; j < kLnTableSize; ++j) {
+    const double c = 1.0 + (double)j / kLnTableSize;
+    tab[j].x = 1.0 / c;
+    tab[j].y = std::log(c);
+  }
+  DeviceGuard dg(device);
+  double2* d = nullptr;
+  ADS_CUDA(cudaMalloc(&d, kLnTableSize * sizeof(double2)));
+  ADS_CUDA(cudaMemcpy(d, tab.data(), kLnTableSize * sizeof(double2), cudaMemcpyHostToDevice));
+  g_ln_tables[device] = d;
+  *out = d;
   return ADS_OK;
 }
 

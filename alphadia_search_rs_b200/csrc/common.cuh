@@ -186,6 +186,48 @@ __device__ __forceinline__ uint32_t grid_find_closest(const GridView& g, float m
 // about 1e-3 of its inputs; see the design notes.)
 __device__ __forceinline__ float ln_rn(float x) { return __double2float_rn(log((double)x)); }
 
+// Table for ln_fast: for j in [0, 256), c_j = 1 + j/256, {1/c_j, ln(c_j)} in double.
+constexpr int kLnTableBits = 8;
+constexpr int kLnTableSize = 1 << kLnTableBits;
+int device_ln_table(int device, const double2** out);
+
+// The same value as ln_rn(x) for every float x, computed faster: x = 2^e * m,
+// m = c_j * (1 + r) with |r| < 2^-8, ln(1 + r) by its Taylor series to r^7, all in
+// double (error below 2^-40 relative).  If the double result lies within a
+// generous margin (2^-38 relative) of a float rounding boundary -- about one input
+// in 2^14 -- ln_rn decides; elsewhere both round to the same float.  `tab` is the
+// table of device_ln_table (usually staged in shared memory).
+__device__ __forceinline__ float ln_fast(float x, const double2* tab) {
+  const uint32_t b = __float_as_uint(x);
+  if (b <= 0x3F800000u || b >= 0x7F800000u) {  // x <= 1, negative, inf or NaN
+    return b == 0x3F800000u ? 0.0f : ln_rn(x);
+  }
+  const int e = (int)(b >> 23) - 127;
+  const uint32_t j = (b >> (23 - kLnTableBits)) & (kLnTableSize - 1);
+  const double m = (double)__uint_as_float((b & 0x007FFFFFu) | 0x3F800000u);
+  const double2 t = tab[j];
+  const double r = fma(m, t.x, -1.0);
+  double p = 1.0 / 7.0;
+  p = fma(p, r, -1.0 / 6.0);
+  p = fma(p, r, 1.0 / 5.0);
+  p = fma(p, r, -1.0 / 4.0);
+  p = fma(p, r, 1.0 / 3.0);
+  p = fma(p, r, -1.0 / 2.0);
+  p = fma(p, r, 1.0);
+  p = p * r;
+  const double ln2 = 0.6931471805599453094172321;
+  const double y = fma((double)e, ln2, t.y + p);
+  const float f = __double2float_rn(y);
+  const uint32_t fb = __float_as_uint(f);  // f is a positive normal float
+  const uint32_t fe = (fb >> 23) & 0xFFu;
+  double half_ulp = __longlong_as_double((long long)(fe - 127 - 24 + 1023) << 52);
+  // below a power of two the spacing (and the distance to the boundary) halves
+  if ((fb & 0x007FFFFFu) == 0 && y < (double)f) half_ulp *= 0.5;
+  const double dist = fabs(y - (double)f);
+  if (half_ulp - dist <= y * 0x1p-38) return ln_rn(x);
+  return f;
+}
+
 // ------------------------------------------------------------- structures
 struct WinInfo {
   float lo, hi;      // isolation window, inclusive at both ends

@@ -249,372 +249,7 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a) {
   }
 }
 
-// ---------------------------------------------------------------- search
-
-struct SearchArgs {
-  int64_t n_prec;
-  const int* nf;
-  const int* cs;
-  const int* ce;
-  const int* nwin;
-  const int* wins;
-  int maxw;
-  const float* fw;
-  const uint32_t* blo;
-  const uint32_t* bhi;
-  int kf;
-  const WinInfo* win;
-  const uint32_t* ss;
-  const uint16_t* cyc;
-  const float* inten;
-  float kw[kMaxHalf + 1];  // kernel taps w[0..h]; w[h] is the centre
-  int h;
-  int k_out;   // candidates kept per precursor
-  int c_max;   // largest cycle range any precursor can have
-  int cp;      // c_max rounded up to 32
-  int gather_mode;
-  int scan_thresh;
-  unsigned int* work;
-  int* err;
-  int* cand_n;
-  float* cand_score;
-  int* cand_center;
-  unsigned long long* stats;  // nullable: [2] fragments [3] entries read [4] accumulated [5] offsets
-};
-
-struct Smem {
-  float* xrow;    // [nw][cp]
-  float* vrow;    // [nw][cp]
-  float* score;   // [cp]
-  uint32_t* bm;   // [nw][bw]
-  float* scr;     // [nw][32]
-  float* mval;    // [mx]
-  int* midx;      // [mx]
-  int* misc;      // [4]
-  int bw, mx;
-};
-
-__host__ __device__ inline int bitmap_words(int cp) { return cp / 32 + 3; }
-__host__ __device__ inline int maxima_cap(int cp) { return cp / 4 + 8; }
-
-__host__ __device__ inline size_t search_smem_bytes(int nw, int cp) {
-  const size_t words = (size_t)nw * cp * 2 + cp + (size_t)nw * bitmap_words(cp) + (size_t)nw * 32 +
-                       2 * (size_t)maxima_cap(cp) + 4;
-  return words * 4;
-}
-
-__device__ __forceinline__ Smem carve(float* base, int nw, int cp) {
-  Smem s;
-  s.bw = bitmap_words(cp);
-  s.mx = maxima_cap(cp);
-  float* q = base;
-  s.xrow = q;
-  q += (size_t)nw * cp;
-  s.vrow = q;
-  q += (size_t)nw * cp;
-  s.score = q;
-  q += cp;
-  s.bm = reinterpret_cast<uint32_t*>(q);
-  q += (size_t)nw * s.bw;
-  s.scr = q;
-  q += (size_t)nw * 32;
-  s.mval = q;
-  q += s.mx;
-  s.midx = reinterpret_cast<int*>(q);
-  q += s.mx;
-  s.misc = reinterpret_cast<int*>(q);
-  return s;
-}
-
-// Adds this chunk's accepted entries to the XIC row in lane (= CSR) order: lanes
-// that hit the same cycle are summed by their lowest lane, one rounded add per
-// entry, exactly like the reference's `dense_xic[c] += intensity`
-// (src/quadrupole_observation/mod.rs:96-105).
-__device__ __forceinline__ void accumulate(bool inc, int cell, float v, int lane, float* row,
-                                           uint32_t* bm, float* scr, unsigned long long& n_acc) {
-  const unsigned act = __ballot_sync(kFull, inc);
-  if (act == 0) return;
-  n_acc += __popc(act);
-  const int key = inc ? cell : (-1 - lane);
-  const unsigned grp = __match_any_sync(kFull, key);
-  scr[lane] = v;
-  __syncwarp();
-  if (inc && lane == __ffs(grp) - 1) {
-    float acc = row[cell];
-    unsigned g = grp;
-    while (g) {
-      const int l = __ffs(g) - 1;
-      acc = __fadd_rn(acc, scr[l]);
-      g &= g - 1;
-    }
-    row[cell] = acc;
-    atomicOr(bm + (cell >> 5), 1u << (cell & 31));
-  }
-  __syncwarp();
-}
-
-// One (fragment, quadrupole window) pair: fill_xic_slice over the fragment's bin
-// range.  Two exact strategies:
-//   scan     read every entry of the contiguous CSR range of the bins and keep
-//            those with start < cycle < stop, plus the last entry at cycle ==
-//            start of each bin (where Rust's binary search lands);
-//   bsearch  per bin, binary-search the first kept entry and the first entry
-//            at or past stop, then read only the kept entries.
-__device__ void gather(const SearchArgs& a, const WinInfo& wi, uint32_t b0, uint32_t b1, int cs,
-                       int ce, int lane, float* row, uint32_t* bm, float* scr,
-                       unsigned long long& n_read, unsigned long long& n_acc,
-                       unsigned long long& n_off, unsigned long long& n_pairs,
-                       unsigned long long& n_bins1) {
-  if (b1 <= b0) return;
-  const uint32_t* ssw = a.ss + wi.ss_off;
-  const uint16_t* cy = a.cyc + wi.base;
-  const float* in = a.inten + wi.base;
-  const int64_t rs = __ldg(ssw + b0), re = __ldg(ssw + b1);
-  n_off += 2;
-  n_pairs += 1;
-  n_bins1 += b1 - b0 + 1;
-  const int64_t n = re - rs;
-  if (n <= 0) return;
-  const bool scan = a.gather_mode == 1 || (a.gather_mode == 0 && n <= a.scan_thresh);
-  if (scan) {
-    n_read += n;
-    for (int64_t q0 = rs; q0 < re; q0 += 32) {
-      const int64_t q = q0 + lane;
-      const bool valid = q < re;
-      const int c = valid ? (int)__ldg(cy + q) : 0;
-      bool inc = valid && c > cs && c < ce;
-      if (valid && c == cs) {
-        const int64_t nxt = q + 1;
-        bool last = nxt == re;
-        if (!last) {
-          // is nxt the first entry of a later bin?  (slice_starts[b] == nxt)
-          uint32_t lo = b0 + 1, hi = b1;
-          while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if ((int64_t)__ldg(ssw + mid) < nxt)
-              lo = mid + 1;
-            else
-              hi = mid;
-          }
-          last = (lo < b1) && ((int64_t)__ldg(ssw + lo) == nxt);
-          if (!last) last = (int)__ldg(cy + nxt) != cs;
-        }
-        inc = last;
-      }
-      const float v = inc ? __ldg(in + q) : 0.0f;
-      accumulate(inc, c - cs, v, lane, row, bm, scr, n_acc);
-    }
-  } else {
-    for (uint32_t bb = b0; bb < b1; bb += 32) {
-      const uint32_t b = bb + lane;
-      const bool vb = b < b1;
-      int64_t pos = 0, cnt = 0;
-      if (vb) {
-        const int64_t s = __ldg(ssw + b), e = __ldg(ssw + b + 1);
-        pos = s + rust_bsearch_u16(cy + s, e - s, cs);
-        const int64_t end = pos + lower_bound_u16(cy + pos, e - pos, ce);
-        cnt = end - pos;
-      }
-      n_off += 2 * __popc(__ballot_sync(kFull, vb));
-      int64_t incl = cnt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int64_t t = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t;
-      }
-      const int64_t total = __shfl_sync(kFull, incl, 31);
-      const int64_t excl = incl - cnt;
-      n_read += total;
-      for (int64_t t0 = 0; t0 < total; t0 += 32) {
-        const int64_t t = t0 + lane;
-        int l = 0;
-#pragma unroll
-        for (int st = 16; st >= 1; st >>= 1) {
-          const int c = l + st;
-          const int64_t ec = __shfl_sync(kFull, excl, c);
-          if (ec <= t) l = c;
-        }
-        const int64_t opos = __shfl_sync(kFull, pos, l);
-        const int64_t oex = __shfl_sync(kFull, excl, l);
-        const bool vt = t < total;
-        const int64_t q = opos + (t - oex);
-        const int c = vt ? (int)__ldg(cy + q) : 0;
-        const float v = vt ? __ldg(in + q) : 0.0f;
-        accumulate(vt, c - cs, v, lane, row, bm, scr, n_acc);
-      }
-    }
-  }
-}
-
-// 2h+1 bitmap bits starting at bit p0.
-__device__ __forceinline__ uint64_t window_bits(const uint32_t* bm, int p0, int nbits) {
-  const int w = p0 >> 5, off = p0 & 31;
-  const uint64_t lo = (uint64_t)bm[w] | ((uint64_t)bm[w + 1] << 32);
-  uint64_t r = lo >> off;
-  if (off) r |= (uint64_t)bm[w + 2] << (64 - off);
-  return r & ((1ull << nbits) - 1);
-}
-
-// convolution_scalar (src/convolution/scalar.rs:5-56) at every output whose
-// 2h+1 window holds a nonzero XIC cell, then ln(conv + 1) * w_f
-// (src/score/scalar.rs:16-22).  Terms whose inputs are both zero add +0 and are
-// skipped; the others are added in the reference's order: centre first, then
-// distance h down to 1 with (left + right) * w[h - d].
-__device__ __forceinline__ void convolve_row(const SearchArgs& a, const float* x,
-                                             const uint32_t* bm, float wf, int C, int lane,
-                                             float* vout) {
-  const int h = a.h;
-  const uint32_t lmask = (1u << h) - 1u;
-  for (int j = lane; j < C; j += 32) {
-    float v = 0.0f;
-    if (j >= h && j < C - h) {
-      const uint64_t m = window_bits(bm, j - h, 2 * h + 1);
-      if (m) {
-        float s = __fadd_rn(0.0f, __fmul_rn(x[j], a.kw[h]));
-        const uint32_t lb = (uint32_t)m & lmask;
-        const uint32_t rb = (uint32_t)(m >> (h + 1)) & lmask;
-        uint32_t D = lb | (__brev(rb) >> (32 - h));
-        while (D) {
-          const int k = __ffs(D) - 1;
-          const int d = h - k;
-          s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[j - d], x[j + d]), a.kw[k]));
-          D &= D - 1;
-        }
-        v = __fmul_rn(ln_rn(__fadd_rn(s, 1.0f)), wf);
-      }
-    }
-    vout[j] = v;
-  }
-}
-
-__global__ void search_kernel(SearchArgs a) {
-  extern __shared__ float smem_raw[];
-  const int nw = blockDim.x >> 5;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  Smem S = carve(smem_raw, nw, a.cp);
-  float* row = S.xrow + (size_t)warp * a.cp;
-  float* vrow = S.vrow + (size_t)warp * a.cp;
-  uint32_t* bm = S.bm + (size_t)warp * S.bw;
-  float* scr = S.scr + warp * 32;
-  unsigned long long n_read = 0, n_acc = 0, n_off = 0, n_frag = 0, n_pairs = 0, n_bins1 = 0;
-
-  for (;;) {
-    if (threadIdx.x == 0) S.misc[0] = (int)atomicAdd(a.work, 1u);
-    __syncthreads();
-    const int64_t p = S.misc[0];
-    __syncthreads();
-    if (p >= a.n_prec) break;
-    const int F = a.nf[p];
-    const int cs = a.cs[p], ce = a.ce[p];
-    const int C = ce - cs;
-    if (F == 0 || C <= 0) {
-      if (threadIdx.x == 0) a.cand_n[p] = 0;
-      continue;
-    }
-    if (C > a.c_max) {
-      if (threadIdx.x == 0) {
-        a.cand_n[p] = 0;
-        atomicOr(a.err, 2);
-      }
-      continue;
-    }
-    const int nwin = a.nwin[p];
-    for (int j = threadIdx.x; j < C; j += blockDim.x) S.score[j] = 0.0f;
-    n_frag += (warp == 0 && lane == 0) ? F : 0;
-
-    for (int r0 = 0; r0 < F; r0 += nw) {
-      const int f = r0 + warp;
-      const int nq = min(nw, F - r0);
-      if (f < F) {
-        for (int j = lane; j < C; j += 32) row[j] = 0.0f;
-        for (int j = lane; j < S.bw; j += 32) bm[j] = 0u;
-        __syncwarp();
-        const int64_t fo = p * a.kf + f;
-        const uint32_t b0 = a.blo[fo], b1 = a.bhi[fo];
-        for (int wi = 0; wi < nwin; ++wi) {
-          const WinInfo w = a.win[a.wins[p * a.maxw + wi]];
-          gather(a, w, b0, b1, cs, ce, lane, row, bm, scr, n_read, n_acc, n_off, n_pairs, n_bins1);
-        }
-        __syncwarp();
-        convolve_row(a, row, bm, a.fw[fo], C, lane, vrow);
-      }
-      __syncthreads();
-      // score[j] += v_f[j] in fragment order (src/score/scalar.rs:16-22)
-      for (int j = threadIdx.x; j < C; j += blockDim.x) {
-        float acc = S.score[j];
-        for (int q = 0; q < nq; ++q) acc = __fadd_rn(acc, S.vrow[(size_t)q * a.cp + j]);
-        S.score[j] = acc;
-      }
-      __syncthreads();
-    }
-
-    // strict 5-point local maxima (src/peak_group_selection/mod.rs:33-43)
-    if (threadIdx.x == 0) S.misc[1] = 0;
-    __syncthreads();
-    for (int i = threadIdx.x + 2; i < C - 2; i += blockDim.x) {
-      const float* sc = S.score;
-      if (sc[i - 2] < sc[i - 1] && sc[i - 1] < sc[i] && sc[i] > sc[i + 1] && sc[i + 1] > sc[i + 2]) {
-        const int k = atomicAdd(&S.misc[1], 1);
-        if (k < S.mx) {
-          S.mval[k] = sc[i];
-          S.midx[k] = i;
-        }
-      }
-    }
-    __syncthreads();
-    // top-K by (value descending, cycle ascending): the reference's stable sort
-    // by value of maxima found in cycle order (src/peak_group_selection/mod.rs:45-61).
-    if (warp == 0) {
-      const int nmax = min(S.misc[1], S.mx);
-      if (S.misc[1] > S.mx && lane == 0) atomicOr(a.err, 4);
-      const int kk = min(a.k_out, nmax);
-      for (int r = 0; r < kk; ++r) {
-        float bv = 0.0f;
-        int bi = -1, bk = -1;
-        for (int k = lane; k < nmax; k += 32) {
-          const float v = S.mval[k];
-          const int i = S.midx[k];
-          if (v != v) continue;  // already taken
-          if (bk < 0 || v > bv || (v == bv && i < bi)) {
-            bv = v;
-            bi = i;
-            bk = k;
-          }
-        }
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-          const float ov = __shfl_xor_sync(kFull, bv, o);
-          const int oi = __shfl_xor_sync(kFull, bi, o);
-          const int ok = __shfl_xor_sync(kFull, bk, o);
-          if (ok >= 0 && (bk < 0 || ov > bv || (ov == bv && oi < bi))) {
-            bv = ov;
-            bi = oi;
-            bk = ok;
-          }
-        }
-        if (lane == 0) {
-          a.cand_score[p * a.k_out + r] = bv;
-          a.cand_center[p * a.k_out + r] = cs + bi;
-          S.mval[bk] = __int_as_float(0x7fc00000);
-        }
-        __syncwarp();
-      }
-      if (lane == 0) a.cand_n[p] = kk;
-    }
-    __syncthreads();
-  }
-  if (a.stats) {
-    // the counters are warp-uniform: count them once per warp
-    if (lane == 0) {
-      atomicAdd(a.stats + 0, n_pairs);
-      atomicAdd(a.stats + 1, n_bins1);
-      atomicAdd(a.stats + 2, n_frag);
-      atomicAdd(a.stats + 3, n_read);
-      atomicAdd(a.stats + 4, n_acc);
-      atomicAdd(a.stats + 5, n_off);
-    }
-  }
-}
+#include "search_kernel.cuh"
 
 // ------------------------------------------------------------ compaction
 
@@ -741,9 +376,13 @@ struct AdsSelection {
   cudaEvent_t* stage_ev = nullptr;  // set of the search being enqueued
 };
 
+// A candidate collection does not depend on the selection that filled it: the
+// search records `done` on the selection's stream, and every later read waits on
+// that event from the collection's own copy stream.
 struct AdsCandidates {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t done = nullptr;
   int64_t cap = 0;
   ads::DevBuf<uint64_t> pidx, rank, center, start, stop;
   ads::DevBuf<float> score;
@@ -751,6 +390,11 @@ struct AdsCandidates {
   ads::DevBuf<int> err_dev;
   int64_t count = 0;
   bool pending = false;
+  ~AdsCandidates() {
+    if (done) cudaEventSynchronize(done);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (done) cudaEventDestroy(done);
+  }
 };
 
 namespace ads {
@@ -806,7 +450,10 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
     return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
   DeviceGuard dg(s->device);
   cudaStream_t st = s->o.stream ? (cudaStream_t)s->o.stream : s->stream;
-  c->stream = st;
+  if (!c->done) ADS_CUDA(cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming));
+  if (!c->copy_stream) ADS_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  // the previous read-out of these buffers must be complete before they are rewritten
+  ADS_CUDA(cudaStreamSynchronize(c->copy_stream));
   const int64_t P = l->n_prec;
   const AdsSelectionParams& prm = s->p;
   const int L = (int)s->kernel.size();
@@ -829,6 +476,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   c->count = 0;
   if (P == 0 || k_out == 0) {
     s->last_launches = 0;
+    ADS_CUDA(cudaEventRecord(c->done, st));
     return ADS_OK;
   }
 
@@ -911,18 +559,34 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
     ++launches;
   }
 
+  // block shape: warps per block (option or default) and how many fragment rows
+  // of the XIC fit in shared memory at once
   int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : 4;
-  nw = std::max(1, std::min(nw, 32));
-  size_t smem = search_smem_bytes(nw, cp);
+  nw = std::max(1, std::min(nw, 8));
   int max_smem = 0;
   ADS_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
-  while (smem > (size_t)max_smem && nw > 1) smem = search_smem_bytes(--nw, cp);
+  const size_t budget = std::min<size_t>((size_t)max_smem, 96 * 1024);
+  int rows = kf;
+  auto plan_bytes = [&](int w, int r) { return (size_t)smem_plan(w, cp, r).total * 4; };
+  while (rows > 1 && plan_bytes(nw, rows) > budget) --rows;
+  while (nw > 1 && plan_bytes(nw, rows) > (size_t)max_smem) --nw;
+  const size_t smem = plan_bytes(nw, rows);
   if (smem > (size_t)max_smem)
     return fail(ADS_ERR_INVALID_ARGUMENT, "RT window too long for shared memory (" +
                                               std::to_string(c_max) + " cycles)");
-  ADS_CUDA(cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const double2* ln_tab = nullptr;
+  ADS_TRY(device_ln_table(s->device, &ln_tab));
+  void (*kern)(SearchArgs);
+  switch (s->h) {
+    case 10: kern = search_kernel<10>; break;
+    case 11: kern = search_kernel<11>; break;
+    case 15: kern = search_kernel<15>; break;
+    case 16: kern = search_kernel<16>; break;
+    default: kern = search_kernel<0>; break;
+  }
+  ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
-  ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel, nw * 32, smem));
+  ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
   if (occ <= 0) return fail(ADS_ERR_INTERNAL, "search kernel cannot be resident");
   int bps = s->o.blocks_per_sm > 0 ? std::min(s->o.blocks_per_sm, occ) : occ;
 
@@ -943,13 +607,15 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   sa.ss = d->slice_starts.p;
   sa.cyc = d->cycles.p;
   sa.inten = d->intens.p;
+  sa.ln_tab = ln_tab;
   for (int k = 0; k <= s->h; ++k) sa.kw[k] = s->kernel[k];
   sa.h = s->h;
   sa.k_out = k_out;
   sa.c_max = (int)c_max;
   sa.cp = cp;
+  sa.rows = rows;
   sa.gather_mode = s->o.gather_mode;
-  sa.scan_thresh = 256;
+  sa.scan_thresh = 32 * kPrefetchChunks;
   sa.work = s->work.p;
   sa.err = c->err_dev.p;
   sa.cand_n = s->cand_n.p;
@@ -959,7 +625,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   if (timed) ADS_CUDA(cudaEventRecord(s->stage_ev[1], st));
   {
     const int64_t blocks = std::min<int64_t>((int64_t)s->num_sms * bps, P);
-    search_kernel<<<(int)blocks, nw * 32, smem, st>>>(sa);
+    kern<<<(int)blocks, nw * 32, smem, st>>>(sa);
     ADS_LAUNCH_CHECK();
     ++launches;
   }
@@ -993,6 +659,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
     ++s->stage_used;
   }
   s->last_launches = launches;
+  ADS_CUDA(cudaEventRecord(c->done, st));
   return ADS_OK;
 }
 
@@ -1001,9 +668,11 @@ int finish(AdsCandidates* c) {
   DeviceGuard dg(c->device);
   int64_t cnt = 0;
   int err = 0;
-  ADS_CUDA(cudaMemcpyAsync(&cnt, c->count_dev.p, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
-  ADS_CUDA(cudaMemcpyAsync(&err, c->err_dev.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  ADS_CUDA(cudaStreamSynchronize(c->stream));
+  ADS_CUDA(cudaStreamWaitEvent(c->copy_stream, c->done, 0));
+  ADS_CUDA(cudaMemcpyAsync(&cnt, c->count_dev.p, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                           c->copy_stream));
+  ADS_CUDA(cudaMemcpyAsync(&err, c->err_dev.p, sizeof(int), cudaMemcpyDeviceToHost, c->copy_stream));
+  ADS_CUDA(cudaStreamSynchronize(c->copy_stream));
   c->pending = false;
   if (err)
     return fail(ADS_ERR_INTERNAL, "search kernel reported internal error flags " + std::to_string(err));
@@ -1160,7 +829,6 @@ int ads_candidates_create(const AdsSelection* s, AdsCandidates** out) {
     if (!s || !out) return fail(ADS_ERR_INVALID_ARGUMENT, "null argument");
     auto c = std::make_unique<AdsCandidates>();
     c->device = s->device;
-    c->stream = s->o.stream ? (cudaStream_t)s->o.stream : s->stream;
     *out = c.release();
     return ADS_OK;
   });
@@ -1224,10 +892,11 @@ int ads_candidates_copy_out(AdsCandidates* c, uint64_t* pidx, uint64_t* rank, fl
                 {center, c->center.p, 8}, {start, c->start.p, 8}, {stop, c->stop.p, 8}};
     for (auto& col : cols)
       if (col.dst)
-        ADS_CUDA(cudaMemcpyAsync(col.dst, col.src, n * col.bytes, cudaMemcpyDeviceToHost, c->stream));
+        ADS_CUDA(cudaMemcpyAsync(col.dst, col.src, n * col.bytes, cudaMemcpyDeviceToHost,
+                                 c->copy_stream));
     for (uint64_t* z : {scan_center, scan_start, scan_stop})
       if (z) std::memset(z, 0, n * 8);
-    ADS_CUDA(cudaStreamSynchronize(c->stream));
+    ADS_CUDA(cudaStreamSynchronize(c->copy_stream));
     return ADS_OK;
   });
 }
@@ -1236,7 +905,6 @@ int ads_candidates_destroy(AdsCandidates* c) {
   return guarded([&] {
     if (!c) return ADS_OK;
     DeviceGuard dg(c->device);
-    if (c->stream) cudaStreamSynchronize(c->stream);
     delete c;
     return ADS_OK;
   });
