@@ -122,6 +122,7 @@ SIGNATURES = {
     "ads_selection_params_default": (None, [C.POINTER(AdsSelectionParams)]),
     "ads_engine_options_default": (None, [C.POINTER(AdsEngineOptions)]),
     "ads_gaussian_kernel": (C.c_int, [f32, f32, i64, f32, vp, i64, C.POINTER(i64)]),
+    "ads_selftest_ln": (C.c_int, [C.c_int, C.c_uint32, C.c_uint32, C.POINTER(i64), C.POINTER(i64)]),
     "ads_selection_create": (C.c_int, [C.POINTER(AdsSelectionParams), C.POINTER(AdsEngineOptions), C.c_int, C.POINTER(vp)]),
     "ads_selection_destroy": (C.c_int, [vp]),
     "ads_selection_kernel": (C.c_int, [vp, vp, i64, C.POINTER(i64)]),

@@ -184,3 +184,43 @@ std::vector<float> gaussian_kernel(float fwhm_rt, float sigma_scale_rt, int64_t 
 }  // namespace ads
 
 extern "C" const char* ads_last_error(void) { return ads::g_last_error.c_str(); }
+
+namespace {
+__global__ void selftest_ln_kernel(uint32_t lo, uint32_t hi, const double2* tab,
+                                   unsigned long long* out) {
+  unsigned long long bad = 0, slow = 0;
+  const uint64_t n = (uint64_t)hi - lo;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const float x = __uint_as_float(lo + (uint32_t)i);
+    bool s = false;
+    const float a = ads::ln_fast(x, tab, &s);
+    const float b = ads::ln_rn(x);
+    bad += __float_as_uint(a) != __float_as_uint(b);
+    slow += s;
+  }
+  atomicAdd(out, bad);
+  atomicAdd(out + 1, slow);
+}
+}  // namespace
+
+extern "C" int ads_selftest_ln(int device, uint32_t lo_bits, uint32_t hi_bits, int64_t* mismatches,
+                               int64_t* slow_path) {
+  using namespace ads;
+  return guarded([&] {
+    if (hi_bits < lo_bits) return fail(ADS_ERR_INVALID_ARGUMENT, "hi_bits < lo_bits");
+    DeviceGuard dg(device);
+    const double2* tab = nullptr;
+    ADS_TRY(device_ln_table(device, &tab));
+    DevBuf<unsigned long long> out;
+    ADS_TRY(out.alloc(2));
+    ADS_CUDA(cudaMemset(out.p, 0, 16));
+    selftest_ln_kernel<<<148 * 16, 256>>>(lo_bits, hi_bits, tab, out.p);
+    ADS_LAUNCH_CHECK();
+    unsigned long long h[2];
+    ADS_CUDA(cudaMemcpy(h, out.p, 16, cudaMemcpyDeviceToHost));
+    if (mismatches) *mismatches = (int64_t)h[0];
+    if (slow_path) *slow_path = (int64_t)h[1];
+    return ADS_OK;
+  });
+}

@@ -197,7 +197,7 @@ int device_ln_table(int device, const double2** out);
 // generous margin (2^-38 relative) of a float rounding boundary -- about one input
 // in 2^14 -- ln_rn decides; elsewhere both round to the same float.  `tab` is the
 // table of device_ln_table (usually staged in shared memory).
-__device__ __forceinline__ float ln_fast(float x, const double2* tab) {
+__device__ __forceinline__ float ln_fast(float x, const double2* tab, bool* slow = nullptr) {
   const uint32_t b = __float_as_uint(x);
   if (b <= 0x3F800000u || b >= 0x7F800000u) {  // x <= 1, negative, inf or NaN
     return b == 0x3F800000u ? 0.0f : ln_rn(x);
@@ -224,7 +224,10 @@ __device__ __forceinline__ float ln_fast(float x, const double2* tab) {
   // below a power of two the spacing (and the distance to the boundary) halves
   if ((fb & 0x007FFFFFu) == 0 && y < (double)f) half_ulp *= 0.5;
   const double dist = fabs(y - (double)f);
-  if (half_ulp - dist <= y * 0x1p-38) return ln_rn(x);
+  if (half_ulp - dist <= y * 0x1p-38) {
+    if (slow) *slow = true;
+    return ln_rn(x);
+  }
   return f;
 }
 

@@ -95,6 +95,13 @@ int ads_dia_copy_observation(const AdsDia* dia, int64_t obs, uint32_t* slice_sta
 int64_t ads_mz_grid_len(void);
 int ads_mz_grid(float* out, int64_t cap);
 
+/* Self-test of the device logarithm (no reference counterpart): evaluates the
+ * search kernel's ln over every float whose bit pattern lies in [lo_bits, hi_bits)
+ * and counts results that differ from ln rounded once from double precision, and
+ * inputs that took the slow path. */
+int ads_selftest_ln(int device, uint32_t lo_bits, uint32_t hi_bits, int64_t* mismatches,
+                    int64_t* slow_path);
+
 /* ---------------------------------------------------------------- SpecLibFlat
  * Replaces SpecLibFlat::from_arrays (src/speclib_flat/mod.rs:100-188): precursor
  * arrays are stably sorted by precursor_idx, fragment arrays keep their order.
