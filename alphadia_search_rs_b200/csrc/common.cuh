@@ -186,6 +186,11 @@ __device__ __forceinline__ uint32_t grid_find_closest(const GridView& g, float m
 // about 1e-3 of its inputs; see the design notes.)
 __device__ __forceinline__ float ln_rn(float x) { return __double2float_rn(log((double)x)); }
 
+// The same, kept out of line for rarely taken paths (keeps hot loops small).
+static __device__ __noinline__ float ln_rn_slow(float x) {
+  return __double2float_rn(log((double)x));
+}
+
 // Table for ln_fast: for j in [0, 256), c_j = 1 + j/256, {1/c_j, ln(c_j)} in double.
 constexpr int kLnTableBits = 8;
 constexpr int kLnTableSize = 1 << kLnTableBits;
@@ -200,7 +205,7 @@ int device_ln_table(int device, const double2** out);
 __device__ __forceinline__ float ln_fast(float x, const double2* tab, bool* slow = nullptr) {
   const uint32_t b = __float_as_uint(x);
   if (b <= 0x3F800000u || b >= 0x7F800000u) {  // x <= 1, negative, inf or NaN
-    return b == 0x3F800000u ? 0.0f : ln_rn(x);
+    return b == 0x3F800000u ? 0.0f : ln_rn_slow(x);
   }
   const int e = (int)(b >> 23) - 127;
   const uint32_t j = (b >> (23 - kLnTableBits)) & (kLnTableSize - 1);
@@ -226,7 +231,7 @@ __device__ __forceinline__ float ln_fast(float x, const double2* tab, bool* slow
   const double dist = fabs(y - (double)f);
   if (half_ulp - dist <= y * 0x1p-38) {
     if (slow) *slow = true;
-    return ln_rn(x);
+    return ln_rn_slow(x);
   }
   return f;
 }

@@ -12,8 +12,9 @@
 //   2. convolve every thread takes strips of 8 outputs of any row: empty input
 //               windows are skipped, single-input windows take one multiply, the
 //               rest run the reference's stencil fully unrolled (H = half width);
-//               then v = ln(conv + 1) * w_f;
-//   3. score    score[j] += v_f[j] in fragment order;
+//               the convolved row is stored;
+//   3. score    score[j] += ln(conv_f[j] + 1) * w_f in fragment order (the logs
+//               run here, balanced over cycles, and only for nonzero values);
 // then maxima and top-K.  All f32 arithmetic is explicitly rounded and in the
 // reference's order, so results equal the reference's except for its logf.
 
@@ -51,7 +52,12 @@ struct SearchArgs {
 };
 
 constexpr int kStrip = 8;           // convolution outputs per work item
-constexpr int kPrefetchChunks = 8;  // 8 x 32 CSR entries read per round trip
+constexpr int kPrefetchChunks = 4;  // 4 x 32 CSR entries read per round trip
+
+// XIC rows are stored skewed, cycle j at j + j/8, so that the threads of a warp,
+// which read strips of 8 consecutive cycles, hit distinct shared-memory banks.
+__host__ __device__ __forceinline__ int xs(int j) { return j + (j >> 3); }
+__host__ __device__ __forceinline__ int row_stride(int cp) { return cp + cp / 8; }
 
 __host__ __device__ inline int bitmap_words(int cp) { return cp / 32 + 3; }
 __host__ __device__ inline int maxima_cap(int cp) { return cp / 4 + 8; }
@@ -72,7 +78,7 @@ __host__ __device__ inline SmemPlan smem_plan(int nw, int cp, int rows) {
   s.kw = o;
   o += 32;
   s.xrow = o;
-  o += rows * cp;
+  o += rows * row_stride(cp);
   s.vrow = o;
   o += rows * cp;
   s.bm = o;
@@ -116,7 +122,7 @@ __device__ __forceinline__ void add_chunk(bool inc, int cell, float v, int lane,
   const bool dup = inc && (tags[cell] != mytag || (old >> 5) == (mytag >> 5));
   if (!__any_sync(kFull, dup)) {
     if (inc) {
-      row[cell] = __fadd_rn(row[cell], v);
+      row[xs(cell)] = __fadd_rn(row[xs(cell)], v);
       atomicOr(bm + (cell >> 5), 1u << (cell & 31));
     }
   } else {
@@ -125,14 +131,14 @@ __device__ __forceinline__ void add_chunk(bool inc, int cell, float v, int lane,
     scr[lane] = v;
     __syncwarp();
     if (inc && lane == __ffs(grp) - 1) {
-      float acc = row[cell];
+      float acc = row[xs(cell)];
       unsigned g = grp;
       while (g) {
         const int l = __ffs(g) - 1;
         acc = __fadd_rn(acc, scr[l]);
         g &= g - 1;
       }
-      row[cell] = acc;
+      row[xs(cell)] = acc;
       atomicOr(bm + (cell >> 5), 1u << (cell & 31));
     }
   }
@@ -271,8 +277,7 @@ __device__ __forceinline__ uint64_t window_bits(const uint32_t* bm, int p0, int 
 // +0 and may be left out without changing a bit, which the sparse paths use.
 template <int H>
 __device__ __forceinline__ void conv_strip(const SearchArgs& a, const float* x, const uint32_t* bm,
-                                           const float* kw_s, const double2* lnt, float wf, int C,
-                                           int j0, float* vout) {
+                                           const float* kw_s, int C, int j0, float* vout) {
   const int h = H > 0 ? H : a.h;
   float out[kStrip];
 #pragma unroll
@@ -285,7 +290,7 @@ __device__ __forceinline__ void conv_strip(const SearchArgs& a, const float* x, 
       if (m != 0) {
         if (__popcll(m) == 1) {
           const int pz = p0 + __ffsll((long long)m) - 1;
-          const float x1 = x[pz];
+          const float x1 = x[xs(pz)];
 #pragma unroll
           for (int i = 0; i < kStrip; ++i) {
             const int j = j0 + i;
@@ -297,7 +302,7 @@ __device__ __forceinline__ void conv_strip(const SearchArgs& a, const float* x, 
 #pragma unroll
           for (int i = 0; i < kStrip + 2 * H; ++i) {
             const int p = p0 + i;
-            xr[i] = (p >= 0 && p < C) ? x[p] : 0.0f;
+            xr[i] = (p >= 0 && p < C) ? x[xs(p)] : 0.0f;
           }
 #pragma unroll
           for (int i = 0; i < kStrip; ++i) {
@@ -316,27 +321,23 @@ __device__ __forceinline__ void conv_strip(const SearchArgs& a, const float* x, 
       for (int j = lo; j < hi; ++j) {
         const uint64_t m = window_bits(bm, j - h, 2 * h + 1);
         if (!m) continue;
-        float s = __fadd_rn(0.0f, __fmul_rn(x[j], kw_s[h]));
+        float s = __fadd_rn(0.0f, __fmul_rn(x[xs(j)], kw_s[h]));
         const uint32_t lb = (uint32_t)m & lmask;
         const uint32_t rb = (uint32_t)(m >> (h + 1)) & lmask;
         uint32_t D = lb | (__brev(rb) >> (32 - h));
         while (D) {
           const int k = __ffs(D) - 1;
           const int d = h - k;
-          s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[j - d], x[j + d]), kw_s[k]));
+          s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[xs(j - d)], x[xs(j + d)]), kw_s[k]));
           D &= D - 1;
         }
         out[j - j0] = s;
       }
     }
   }
-  float v[kStrip];
-#pragma unroll
-  for (int i = 0; i < kStrip; ++i)
-    v[i] = out[i] != 0.0f ? __fmul_rn(ln_fast(__fadd_rn(out[i], 1.0f), lnt), wf) : 0.0f;
   float4* o4 = reinterpret_cast<float4*>(vout + j0);
-  o4[0] = make_float4(v[0], v[1], v[2], v[3]);
-  o4[1] = make_float4(v[4], v[5], v[6], v[7]);
+  o4[0] = make_float4(out[0], out[1], out[2], out[3]);
+  o4[1] = make_float4(out[4], out[5], out[6], out[7]);
 }
 
 template <int H>
@@ -394,7 +395,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
       // zero the rows and their bitmaps
       {
         float4* x4 = reinterpret_cast<float4*>(xrow);
-        const int n4 = nr * cp / 4;
+        const int n4 = nr * row_stride(cp) / 4;
         for (int i = threadIdx.x; i < n4; i += blockDim.x) x4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         for (int i = threadIdx.x; i < nr * P.bw; i += blockDim.x) bm[i] = 0u;
       }
@@ -433,7 +434,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
             k.off += 2;
             k.pairs += 1;
             k.bins1 += qb1 - qb0 + 1;
-            gather_pair(a, w, qb0, qb1, qrs, qre, cs, ce, lane, xrow + (size_t)fl * cp,
+            gather_pair(a, w, qb0, qb1, qrs, qre, cs, ce, lane, xrow + (size_t)fl * row_stride(cp),
                         bm + fl * P.bw, tags, scr, seq, k);
           }
         }
@@ -443,14 +444,19 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
       for (int it = threadIdx.x; it < nr * nstrips; it += blockDim.x) {
         const int fl = it / nstrips;
         const int j0 = (it - fl * nstrips) * kStrip;
-        conv_strip<H>(a, xrow + (size_t)fl * cp, bm + fl * P.bw, kw_s, lnt,
-                      a.fw[p * a.kf + r0 + fl], C, j0, vrow + (size_t)fl * cp);
+        conv_strip<H>(a, xrow + (size_t)fl * row_stride(cp), bm + fl * P.bw, kw_s, C, j0,
+                      vrow + (size_t)fl * cp);
       }
       __syncthreads();
-      // ---- score[j] += v_f[j] in fragment order (src/score/scalar.rs:16-22)
+      // ---- score[j] += ln(conv_f[j] + 1) * w_f in fragment order
+      // (src/score/scalar.rs:16-22); a zero conv adds ln(1) * w = +0 and is skipped
+      const float* fw = a.fw + p * a.kf + r0;
       for (int j = threadIdx.x; j < C; j += blockDim.x) {
         float acc = r0 == 0 ? 0.0f : score[j];
-        for (int q = 0; q < nr; ++q) acc = __fadd_rn(acc, vrow[(size_t)q * cp + j]);
+        for (int q = 0; q < nr; ++q) {
+          const float c = vrow[(size_t)q * cp + j];
+          if (c != 0.0f) acc = __fadd_rn(acc, __fmul_rn(ln_fast(__fadd_rn(c, 1.0f), lnt), __ldg(fw + q)));
+        }
         score[j] = acc;
       }
       __syncthreads();
