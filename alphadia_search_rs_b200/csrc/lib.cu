@@ -75,7 +75,7 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
 
   // validation on host copies of the small per-precursor arrays
   std::vector<uint64_t> fs, fe;
-  std::vector<float> prt, tol, fmz_h;
+  std::vector<float> prt, tol;
   ADS_TRY(host_copy(a->flat_frag_start_idx, P, L, fs));
   ADS_TRY(host_copy(a->flat_frag_stop_idx, P, L, fe));
   ADS_TRY(host_copy(a->precursor_rt, P, L, prt));
@@ -98,10 +98,6 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
       if (std::isfinite(v)) lib->max_tol = std::max(lib->max_tol, v);
       else if (!std::isnan(v)) lib->max_tol = INFINITY;
   }
-  ADS_TRY(host_copy(a->fragment_mz, NF, L, fmz_h));
-  for (int64_t i = 0; i < NF; ++i)
-    if (std::isnan(fmz_h[i]))
-      return fail(ADS_ERR_INVALID_ARGUMENT, "fragment " + std::to_string(i) + ": m/z is NaN");
 
   cudaStream_t st;
   ADS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));

@@ -142,12 +142,57 @@ struct PrepArgs {
   int* err;
 };
 
-// src/speclib_flat/mod.rs:240-345 (non_zero and y1 filters, top-k by intensity,
-// sort by fragment m/z; ties go to the lower library position) followed by the
-// ppm bin range of src/quadrupole_observation/mod.rs:79-83 + src/mz_index/mod.rs:95-127.
+// Fragment m/z ordering key: NaN sorts after every number (ties by library
+// position), so the output positions always form a permutation.
+__device__ __forceinline__ float mz_key(float m) { return m != m ? INFINITY : m; }
+
+// The ppm bin range of one kept fragment (src/quadrupole_observation/mod.rs:79-83,
+// src/mz_index/mod.rs:95-127), stored at its position in m/z order.
+__device__ __forceinline__ void write_fragment(const PrepArgs& a, int64_t p, int pos, float mz,
+                                               float w) {
+  const float delta = __fmul_rn(__fmul_rn(mz, a.mass_tol), 1e-6f);
+  const float lo = __fsub_rn(mz, delta), hi = __fadd_rn(mz, delta);
+  const uint32_t b0 = grid_lower_bound(a.g, lo);
+  const uint32_t b1 = max(b0, grid_upper_bound(a.g, hi));
+  const int64_t o = p * a.kf + pos;
+  a.fw[o] = w;
+  a.blo[o] = b0;
+  a.bhi[o] = b1;
+}
+
+// get_precursor_filtered / filter_sort_fragments (src/speclib_flat/mod.rs:240-345,
+// 388-456): non_zero and y1 filters, top-k by intensity, sort by fragment m/z;
+// ties go to the lower library position.
 __device__ int select_fragments(const PrepArgs& a, int64_t p, int lane, uint8_t* keep) {
   const int64_t s = (int64_t)a.fstart[p];
   const int64_t n = (int64_t)a.fstop[p] - s;
+  if (n <= 32) {
+    // one fragment per lane; rankings through shuffles
+    const bool have = lane < n;
+    const float I = have ? __ldg(a.fint + s + lane) : 0.0f;
+    bool k = have && (I > 0.0f) && !(__ldg(a.ftype + s + lane) == 121 && __ldg(a.fnum + s + lane) == 1);
+    unsigned km = __ballot_sync(kFull, k);
+    if (__popc(km) > a.top_k) {
+      const float ik = k ? I : -1.0f;
+      int rank = 0;
+      for (int j = 0; j < (int)n; ++j) {
+        const float J = __shfl_sync(kFull, ik, j);
+        rank += (J > ik) || (J == ik && j < lane);
+      }
+      k = k && rank < a.top_k;
+      km = __ballot_sync(kFull, k);
+    }
+    const float mz = have ? __ldg(a.fmz + s + lane) : 0.0f;
+    const float key = mz_key(mz);
+    int pos = 0;
+    for (int j = 0; j < (int)n; ++j) {
+      const float m = __shfl_sync(kFull, key, j);
+      if ((km >> j) & 1u) pos += (m < key) || (m == key && j < lane);
+    }
+    if (k) write_fragment(a, p, pos, mz, I);
+    __syncwarp();
+    return __popc(km);
+  }
   int nk = 0;
   for (int64_t i0 = 0; i0 < n; i0 += 32) {
     const int64_t i = i0 + lane;
@@ -183,20 +228,14 @@ __device__ int select_fragments(const PrepArgs& a, int64_t p, int lane, uint8_t*
     const int64_t i = i0 + lane;
     if (i < n && keep[i] >= need) {
       const float mz = __ldg(a.fmz + s + i);
+      const float key = mz_key(mz);
       int pos = 0;
       for (int64_t j = 0; j < n; ++j) {
         if (keep[j] < need) continue;
-        const float m = __ldg(a.fmz + s + j);
-        pos += (m < mz) || (m == mz && j < i);
+        const float m = mz_key(__ldg(a.fmz + s + j));
+        pos += (m < key) || (m == key && j < i);
       }
-      const float delta = __fmul_rn(__fmul_rn(mz, a.mass_tol), 1e-6f);
-      const float lo = __fsub_rn(mz, delta), hi = __fadd_rn(mz, delta);
-      const uint32_t b0 = grid_lower_bound(a.g, lo);
-      const uint32_t b1 = max(b0, grid_upper_bound(a.g, hi));
-      const int64_t o = p * a.kf + pos;
-      a.fw[o] = __ldg(a.fint + s + i);
-      a.blo[o] = b0;
-      a.bhi[o] = b1;
+      write_fragment(a, p, pos, mz, __ldg(a.fint + s + i));
     }
   }
   __syncwarp();
@@ -463,6 +502,9 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   const float tol_max = l->has_tol ? std::max(l->max_tol, 0.0f) : prm.rt_tolerance;
   const int64_t c_max = std::max<int64_t>(1, max_cycle_span(d->rt, d->delta_t, tol_max, prm.kernel_size));
   const int cp = (int)((c_max + 31) / 32 * 32);
+  if (cp > (1 << kListRowShift))
+    return fail(ADS_ERR_INVALID_ARGUMENT, "RT windows longer than 2048 cycles are not supported (" +
+                                              std::to_string(c_max) + " cycles)");
   const int k_out = (int)std::max<int64_t>(0, std::min<int64_t>(prm.candidate_count, maxima_cap(cp)));
   const int kf = (int)std::max<int64_t>(1, std::min<int64_t>(prm.top_k_fragments, l->max_frag));
   const int maxw = std::max(1, d->max_overlap);
@@ -615,7 +657,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   sa.cp = cp;
   sa.rows = rows;
   sa.gather_mode = s->o.gather_mode;
-  sa.scan_thresh = 32 * kPrefetchChunks;
+  sa.scan_thresh = 4 * 32 * kPrefetchChunks;
   sa.work = s->work.p;
   sa.err = c->err_dev.p;
   sa.cand_n = s->cand_n.p;

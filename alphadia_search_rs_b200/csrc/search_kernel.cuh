@@ -7,14 +7,16 @@
 // `rows` fragments (one round when the whole XIC fits in shared memory):
 //   1. gather   warps take fragments round-robin; per (fragment, window) the CSR
 //               offsets of all the warp's pairs are fetched together, then up to
-//               256 entries of a bin range are read in one round trip and added to
+//               128 entries of a bin range are read in one round trip and added to
 //               the fragment's XIC row in CSR order;
-//   2. convolve every thread takes strips of 8 outputs of any row: empty input
-//               windows are skipped, single-input windows take one multiply, the
-//               rest run the reference's stencil fully unrolled (H = half width);
-//               the convolved row is stored;
-//   3. score    score[j] += ln(conv_f[j] + 1) * w_f in fragment order (the logs
-//               run here, balanced over cycles, and only for nonzero values);
+//   2. list     the outputs whose 2h+1 input window holds a nonzero cell (the
+//               bitmap of touched cells dilated by h, inside the valid region) are
+//               collected into a list; every other output is exactly zero;
+//   3. convolve every thread takes list entries: single-input windows take one
+//               multiply, the others run the reference's stencil (fully unrolled
+//               for the common half widths);
+//   4. score    score[j] += ln(conv_f[j] + 1) * w_f in fragment order (logs only
+//               for nonzero values);
 // then maxima and top-K.  All f32 arithmetic is explicitly rounded and in the
 // reference's order, so results equal the reference's except for its logf.
 
@@ -51,20 +53,21 @@ struct SearchArgs {
   unsigned long long* stats;  // nullable
 };
 
-constexpr int kStrip = 8;           // convolution outputs per work item
 constexpr int kPrefetchChunks = 4;  // 4 x 32 CSR entries read per round trip
+constexpr int kListRowShift = 11;   // list entry = row << 11 | cycle (cycle < 2048)
 
-// XIC rows are stored skewed, cycle j at j + j/8, so that the threads of a warp,
-// which read strips of 8 consecutive cycles, hit distinct shared-memory banks.
+// XIC rows are stored skewed, cycle j at j + j/8, so that reads of neighbouring
+// cycles by neighbouring threads spread over the shared-memory banks.
 __host__ __device__ __forceinline__ int xs(int j) { return j + (j >> 3); }
 __host__ __device__ __forceinline__ int row_stride(int cp) { return cp + cp / 8; }
 
 __host__ __device__ inline int bitmap_words(int cp) { return cp / 32 + 3; }
 __host__ __device__ inline int maxima_cap(int cp) { return cp / 4 + 8; }
 
-// Shared-memory plan, in 4-byte words.
+// Shared-memory plan, in 4-byte words.  The per-warp duplicate tags of the gather
+// and the convolved rows of the later phases share one region.
 struct SmemPlan {
-  int ln, kw, xrow, vrow, bm, tags, scr, score, mval, midx, misc, total;
+  int ln, kw, xrow, vrow, tags, list, bm, scr, score, mval, midx, misc, total;
   int bw, mx;
 };
 
@@ -80,11 +83,12 @@ __host__ __device__ inline SmemPlan smem_plan(int nw, int cp, int rows) {
   s.xrow = o;
   o += rows * row_stride(cp);
   s.vrow = o;
-  o += rows * cp;
+  s.tags = o;
+  o += (rows > nw ? rows : nw) * cp;
+  s.list = o;
+  o += (rows * cp + 1) / 2;  // u16 entries
   s.bm = o;
   o += rows * s.bw;
-  s.tags = o;
-  o += nw * cp;
   s.scr = o;
   o += nw * 32;
   s.score = o;
@@ -270,74 +274,55 @@ __device__ __forceinline__ uint64_t window_bits(const uint32_t* bm, int p0, int 
   return r << shift;
 }
 
-// Convolution of one strip of kStrip outputs of one XIC row
-// (convolution_scalar, src/convolution/scalar.rs:30-50) followed by
-// ln(conv + 1) * w_f (src/score/scalar.rs:16-22).  Output j sums, in order,
-// x[j]*w[h] and (x[j-d] + x[j+d]) * w[h-d] for d = h..1; inputs that are zero add
-// +0 and may be left out without changing a bit, which the sparse paths use.
+
+// Active outputs of one 32-cycle word of a row: the touched-cell bitmap dilated
+// by h (cycle j is active if a touched cell lies in [j - h, j + h]), limited to the
+// valid region [h, C - h) where the reference computes anything.
+__device__ __forceinline__ uint32_t active_word(const uint32_t* bm, int w, int h, int C) {
+  const uint32_t c = bm[w], p = w > 0 ? bm[w - 1] : 0u, n = bm[w + 1];
+  uint32_t act = c;
+  for (int d = 1; d <= h; ++d) act |= (c << d) | (p >> (32 - d)) | (c >> d) | (n << (32 - d));
+  const int j0 = w * 32;
+  const int lo = max(h - j0, 0), hi = min(C - h - j0, 32);  // valid bit range [lo, hi)
+  if (hi <= lo) return 0u;
+  const uint32_t upper = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
+  const uint32_t lower = (1u << lo) - 1u;
+  return act & upper & ~lower;
+}
+
+// One output of convolution_scalar (src/convolution/scalar.rs:30-50): x[j]*w[h]
+// first, then (x[j-d] + x[j+d]) * w[h-d] for d = h..1.  Inputs that are zero add
+// +0, so a window with a single nonzero input reduces to that input times its
+// tap, exactly.
 template <int H>
-__device__ __forceinline__ void conv_strip(const SearchArgs& a, const float* x, const uint32_t* bm,
-                                           const float* kw_s, int C, int j0, float* vout) {
+__device__ __forceinline__ float conv_output(const SearchArgs& a, const float* x,
+                                             const uint32_t* bm, const float* kw_s, int j) {
   const int h = H > 0 ? H : a.h;
-  float out[kStrip];
-#pragma unroll
-  for (int i = 0; i < kStrip; ++i) out[i] = 0.0f;
-  const int lo = max(j0, h), hi = min(j0 + kStrip, C - h);  // valid outputs [lo, hi)
-  if (lo < hi) {
-    if (H > 0) {
-      const int p0 = j0 - H;
-      const uint64_t m = window_bits(bm, p0, kStrip + 2 * H);
-      if (m != 0) {
-        if (__popcll(m) == 1) {
-          const int pz = p0 + __ffsll((long long)m) - 1;
-          const float x1 = x[xs(pz)];
-#pragma unroll
-          for (int i = 0; i < kStrip; ++i) {
-            const int j = j0 + i;
-            const int d = abs(pz - j);
-            if (j >= lo && j < hi && d <= H) out[i] = __fmul_rn(x1, kw_s[H - d]);
-          }
-        } else {
-          float xr[kStrip + 2 * (H > 0 ? H : 1)];
-#pragma unroll
-          for (int i = 0; i < kStrip + 2 * H; ++i) {
-            const int p = p0 + i;
-            xr[i] = (p >= 0 && p < C) ? x[xs(p)] : 0.0f;
-          }
-#pragma unroll
-          for (int i = 0; i < kStrip; ++i) {
-            float s = __fadd_rn(0.0f, __fmul_rn(xr[i + H], a.kw[H]));
-#pragma unroll
-            for (int k = 0; k < H; ++k)
-              s = __fadd_rn(s, __fmul_rn(__fadd_rn(xr[i + k], xr[i + 2 * H - k]), a.kw[k]));
-            const int j = j0 + i;
-            out[i] = (j >= lo && j < hi) ? s : 0.0f;
-          }
-        }
-      }
-    } else {
-      // any half width: per output, only the nonzero tap pairs, in the reference order
-      const uint32_t lmask = (1u << h) - 1u;
-      for (int j = lo; j < hi; ++j) {
-        const uint64_t m = window_bits(bm, j - h, 2 * h + 1);
-        if (!m) continue;
-        float s = __fadd_rn(0.0f, __fmul_rn(x[xs(j)], kw_s[h]));
-        const uint32_t lb = (uint32_t)m & lmask;
-        const uint32_t rb = (uint32_t)(m >> (h + 1)) & lmask;
-        uint32_t D = lb | (__brev(rb) >> (32 - h));
-        while (D) {
-          const int k = __ffs(D) - 1;
-          const int d = h - k;
-          s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[xs(j - d)], x[xs(j + d)]), kw_s[k]));
-          D &= D - 1;
-        }
-        out[j - j0] = s;
-      }
-    }
+  const uint64_t m = window_bits(bm, j - h, 2 * h + 1);
+  if (__popcll(m) == 1) {
+    const int d = abs(__ffsll((long long)m) - 1 - h);
+    return __fmul_rn(x[xs(j - h + __ffsll((long long)m) - 1)], kw_s[h - d]);
   }
-  float4* o4 = reinterpret_cast<float4*>(vout + j0);
-  o4[0] = make_float4(out[0], out[1], out[2], out[3]);
-  o4[1] = make_float4(out[4], out[5], out[6], out[7]);
+  if (H > 0) {
+    float s = __fadd_rn(0.0f, __fmul_rn(x[xs(j)], a.kw[H]));
+#pragma unroll
+    for (int k = 0; k < H; ++k)
+      s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[xs(j - H + k)], x[xs(j + H - k)]), a.kw[k]));
+    return s;
+  }
+  // any half width: only the nonzero tap pairs, in the reference order
+  float s = __fadd_rn(0.0f, __fmul_rn(x[xs(j)], kw_s[h]));
+  const uint32_t lmask = (1u << h) - 1u;
+  const uint32_t lb = (uint32_t)m & lmask;
+  const uint32_t rb = (uint32_t)(m >> (h + 1)) & lmask;
+  uint32_t D = lb | (__brev(rb) >> (32 - h));
+  while (D) {
+    const int k = __ffs(D) - 1;
+    const int d = h - k;
+    s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[xs(j - d)], x[xs(j + d)]), kw_s[k]));
+    D &= D - 1;
+  }
+  return s;
 }
 
 template <int H>
@@ -351,19 +336,21 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
   float* kw_s = smem_raw + P.kw;
   float* xrow = smem_raw + P.xrow;
   float* vrow = smem_raw + P.vrow;
-  uint32_t* bm = sw + P.bm;
   uint32_t* tags = sw + P.tags + warp * a.cp;
+  uint16_t* list = reinterpret_cast<uint16_t*>(sw + P.list);
+  uint32_t* bm = sw + P.bm;
   float* scr = smem_raw + P.scr + warp * 32;
   float* score = smem_raw + P.score;
   float* mval = smem_raw + P.mval;
   int* midx = reinterpret_cast<int*>(smem_raw + P.midx);
   int* misc = reinterpret_cast<int*>(smem_raw + P.misc);
   const int cp = a.cp;
+  const int h = H > 0 ? H : a.h;
+  const int nwords = cp / 32;
+  const int n_union = (a.rows > nw ? a.rows : nw) * cp;
 
   for (int i = threadIdx.x; i < kLnTableSize; i += blockDim.x) lnt[i] = a.ln_tab[i];
   for (int i = threadIdx.x; i <= a.h; i += blockDim.x) kw_s[i] = a.kw[i];
-  for (int i = threadIdx.x; i < nw * cp; i += blockDim.x) sw[P.tags + i] = 0u;
-  uint32_t seq = 1;
   Counters k;
 
   for (;;) {
@@ -387,21 +374,25 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
       continue;
     }
     const int nwin = a.nwin[p];
-    const int nstrips = (C + kStrip - 1) / kStrip;
     if (warp == 0 && lane == 0) k.frag += F;
 
     for (int r0 = 0; r0 < F; r0 += a.rows) {
       const int nr = min(a.rows, F - r0);
-      // zero the rows and their bitmaps
+      // zero the XIC rows, the convolved rows (which also clears the gather tags)
+      // and the bitmaps
       {
         float4* x4 = reinterpret_cast<float4*>(xrow);
-        const int n4 = nr * row_stride(cp) / 4;
-        for (int i = threadIdx.x; i < n4; i += blockDim.x) x4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        const int nx4 = nr * row_stride(cp) / 4;
+        for (int i = threadIdx.x; i < nx4; i += blockDim.x) x4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4* v4 = reinterpret_cast<float4*>(vrow);
+        for (int i = threadIdx.x; i < n_union / 4; i += blockDim.x) v4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         for (int i = threadIdx.x; i < nr * P.bw; i += blockDim.x) bm[i] = 0u;
+        if (threadIdx.x == 0) misc[2] = 0;
       }
       __syncthreads();
-      // ---- gather: this warp's rows, all their windows
+      // ---- 1. gather: this warp's rows, all their windows
       {
+        uint32_t seq = 1;
         const int my_rows = nr > warp ? (nr - warp + nw - 1) / nw : 0;
         const int n_pairs = my_rows * nwin;
         for (int pb = 0; pb < n_pairs; pb += 32) {
@@ -440,15 +431,32 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
         }
       }
       __syncthreads();
-      // ---- convolution + log, strips of all rows of the round
-      for (int it = threadIdx.x; it < nr * nstrips; it += blockDim.x) {
-        const int fl = it / nstrips;
-        const int j0 = (it - fl * nstrips) * kStrip;
-        conv_strip<H>(a, xrow + (size_t)fl * row_stride(cp), bm + fl * P.bw, kw_s, C, j0,
-                      vrow + (size_t)fl * cp);
+      // ---- 2. list of the outputs with a nonzero input window
+      for (int it = threadIdx.x; it < nr * nwords; it += blockDim.x) {
+        const int fl = it / nwords, w = it - fl * nwords;
+        uint32_t act = active_word(bm + fl * P.bw, w, h, C);
+        if (act) {
+          int pos = atomicAdd(&misc[2], __popc(act));
+          while (act) {
+            const int b = __ffs(act) - 1;
+            list[pos++] = (uint16_t)((fl << kListRowShift) | (w * 32 + b));
+            act &= act - 1;
+          }
+        }
+      }
+      // the tags region becomes the convolved rows: clear what the gather left
+      for (int i = threadIdx.x; i < nw * cp; i += blockDim.x) vrow[i] = 0.0f;
+      __syncthreads();
+      // ---- 3. convolution of the listed outputs
+      const int n_list = misc[2];
+      for (int it = threadIdx.x; it < n_list; it += blockDim.x) {
+        const int e = list[it];
+        const int fl = e >> kListRowShift, j = e & ((1 << kListRowShift) - 1);
+        vrow[(size_t)fl * cp + j] =
+            conv_output<H>(a, xrow + (size_t)fl * row_stride(cp), bm + fl * P.bw, kw_s, j);
       }
       __syncthreads();
-      // ---- score[j] += ln(conv_f[j] + 1) * w_f in fragment order
+      // ---- 4. score[j] += ln(conv_f[j] + 1) * w_f in fragment order
       // (src/score/scalar.rs:16-22); a zero conv adds ln(1) * w = +0 and is skipped
       const float* fw = a.fw + p * a.kf + r0;
       for (int j = threadIdx.x; j < C; j += blockDim.x) {

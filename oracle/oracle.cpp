@@ -318,7 +318,10 @@ std::vector<int64_t> filter_sort_fragments(int64_t n, const float* mz, const flo
     keep.resize((size_t)k);
     std::sort(keep.begin(), keep.end());
   }
-  std::stable_sort(keep.begin(), keep.end(), [&](int64_t a, int64_t b) { return mz[a] < mz[b]; });
+  // Rust's sort_by with partial_cmp().unwrap_or(Equal) leaves NaN placement
+  // implementation defined; here NaN sorts after every number (stable).
+  auto key = [&](int64_t i) { return std::isnan(mz[i]) ? INFINITY : mz[i]; };
+  std::stable_sort(keep.begin(), keep.end(), [&](int64_t a, int64_t b) { return key(a) < key(b); });
   return keep;
 }
 
