@@ -271,11 +271,17 @@ struct AdsLib {
   int device = 0;
   int64_t n_prec = 0, n_frag = 0;
   int64_t max_frag = 0;  // max fragments of one precursor
-  ads::DevBuf<uint64_t> pidx;    // sorted precursor_idx
-  ads::DevBuf<float> pmz, prt, ptol;
-  ads::DevBuf<uint64_t> fstart, fstop;
-  ads::DevBuf<float> fmz, fint;
-  ads::DevBuf<uint8_t> fnum, ftype;
+  ads::DevBuf<char> arena;  // every array below lives in this one allocation
+  uint64_t* pidx_p = nullptr;  // precursor arrays, sorted by precursor_idx
+  float* pmz_p = nullptr;
+  float* prt_p = nullptr;
+  float* ptol_p = nullptr;     // optional per-precursor RT half-window
+  uint64_t* fstart_p = nullptr;
+  uint64_t* fstop_p = nullptr;
+  float* fmz_p = nullptr;      // fragment arrays, input order
+  float* fint_p = nullptr;
+  uint8_t* fnum_p = nullptr;
+  uint8_t* ftype_p = nullptr;
   bool has_tol = false;
   float max_tol = 0.0f;
 };

@@ -1,6 +1,7 @@
 // SpecLibFlat on the device (SpecLibFlat::from_arrays, src/speclib_flat/mod.rs:100-188).
 // Precursor arrays are stably sorted by precursor_idx; fragment arrays keep their
-// order and are addressed through flat_frag_start/stop_idx.
+// order and are addressed through flat_frag_start/stop_idx.  All device arrays of a
+// library live in one allocation.
 #include <cub/cub.cuh>
 
 #include <cmath>
@@ -20,40 +21,52 @@ __global__ void gather_kernel(int64_t n, const uint32_t* __restrict__ perm,
     dst[i] = src[perm[i]];
 }
 
+__global__ void iota_kernel(int64_t n, uint32_t* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)i;
+}
+
+// Bump allocator over one device allocation (256-byte aligned pieces).
+struct Carver {
+  char* base = nullptr;
+  size_t off = 0;
+  template <class T>
+  T* take(int64_t n) {
+    T* p = reinterpret_cast<T*>(base + off);
+    off += ((size_t)std::max<int64_t>(n, 1) * sizeof(T) + 255) / 256 * 256;
+    return p;
+  }
+};
+
 template <class T>
-int upload(DevBuf<T>& dst, const T* src, int64_t n, int loc, cudaStream_t st) {
-  ADS_TRY(dst.alloc((size_t)std::max<int64_t>(n, 1)));
+int copy_in(T* dst, const T* src, int64_t n, int loc, cudaStream_t st) {
   if (n == 0) return ADS_OK;
   if (!src) return fail(ADS_ERR_INVALID_ARGUMENT, "null array pointer");
-  ADS_CUDA(cudaMemcpyAsync(dst.p, src, (size_t)n * sizeof(T),
+  ADS_CUDA(cudaMemcpyAsync(dst, src, (size_t)n * sizeof(T),
                            loc == ADS_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                            st));
   return ADS_OK;
 }
 
+// Host view of a small per-precursor array: the caller's memory when it is on the
+// host, a copy when it is on the device.
 template <class T>
-int permute(DevBuf<T>& buf, const uint32_t* perm, int64_t n, cudaStream_t st) {
-  if (n == 0) return ADS_OK;
-  DevBuf<T> out;
-  ADS_TRY(out.alloc((size_t)n));
-  gather_kernel<T><<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(n, perm, buf.p,
-                                                                                   out.p);
-  ADS_LAUNCH_CHECK();
-  ADS_CUDA(cudaStreamSynchronize(st));
-  buf = std::move(out);
+int host_view(const T* src, int64_t n, int loc, std::vector<T>& store, const T** out) {
+  if (n > 0 && !src) return fail(ADS_ERR_INVALID_ARGUMENT, "null array pointer");
+  if (loc == ADS_MEM_HOST) {
+    *out = src;
+    return ADS_OK;
+  }
+  store.resize((size_t)n);
+  if (n) ADS_CUDA(cudaMemcpy(store.data(), src, (size_t)n * sizeof(T), cudaMemcpyDeviceToHost));
+  *out = store.data();
   return ADS_OK;
 }
 
 template <class T>
-int host_copy(const T* src, int64_t n, int loc, std::vector<T>& dst) {
-  dst.resize((size_t)n);
-  if (n == 0) return ADS_OK;
-  if (!src) return fail(ADS_ERR_INVALID_ARGUMENT, "null array pointer");
-  if (loc == ADS_MEM_DEVICE)
-    ADS_CUDA(cudaMemcpy(dst.data(), src, (size_t)n * sizeof(T), cudaMemcpyDeviceToHost));
-  else
-    std::memcpy(dst.data(), src, (size_t)n * sizeof(T));
-  return ADS_OK;
+void launch_gather(int64_t n, const uint32_t* perm, const T* src, T* dst, cudaStream_t st) {
+  gather_kernel<T><<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(n, perm, src, dst);
 }
 
 int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
@@ -73,12 +86,14 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
   DeviceGuard dg(device);
   const int L = a->location;
 
-  // validation on host copies of the small per-precursor arrays
-  std::vector<uint64_t> fs, fe;
-  std::vector<float> prt, tol;
-  ADS_TRY(host_copy(a->flat_frag_start_idx, P, L, fs));
-  ADS_TRY(host_copy(a->flat_frag_stop_idx, P, L, fe));
-  ADS_TRY(host_copy(a->precursor_rt, P, L, prt));
+  // validation of the per-precursor arrays (the reference panics on these)
+  std::vector<uint64_t> fs_store, fe_store;
+  std::vector<float> rt_store, tol_store;
+  const uint64_t *fs = nullptr, *fe = nullptr;
+  const float *prt = nullptr, *tol = nullptr;
+  ADS_TRY(host_view(a->flat_frag_start_idx, P, L, fs_store, &fs));
+  ADS_TRY(host_view(a->flat_frag_stop_idx, P, L, fe_store, &fe));
+  ADS_TRY(host_view(a->precursor_rt, P, L, rt_store, &prt));
   auto lib = std::make_unique<AdsLib>();
   lib->device = device;
   lib->n_prec = P;
@@ -92,11 +107,15 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     lib->max_frag = std::max<int64_t>(lib->max_frag, (int64_t)(fe[i] - fs[i]));
   }
   if (a->precursor_rt_tolerance) {
-    ADS_TRY(host_copy(a->precursor_rt_tolerance, P, L, tol));
+    ADS_TRY(host_view(a->precursor_rt_tolerance, P, L, tol_store, &tol));
     lib->has_tol = true;
-    for (float v : tol)
-      if (std::isfinite(v)) lib->max_tol = std::max(lib->max_tol, v);
-      else if (!std::isnan(v)) lib->max_tol = INFINITY;
+    for (int64_t i = 0; i < P; ++i) {
+      const float v = tol[i];
+      if (std::isfinite(v))
+        lib->max_tol = std::max(lib->max_tol, v);
+      else if (!std::isnan(v))
+        lib->max_tol = INFINITY;
+    }
   }
 
   cudaStream_t st;
@@ -106,41 +125,79 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     ~StreamGuard() { cudaStreamDestroy(s); }
   } sg{st};
 
-  ADS_TRY(upload(lib->pidx, a->precursor_idx, P, L, st));
-  ADS_TRY(upload(lib->pmz, a->precursor_mz, P, L, st));
-  ADS_TRY(upload(lib->prt, a->precursor_rt, P, L, st));
-  ADS_TRY(upload(lib->fstart, a->flat_frag_start_idx, P, L, st));
-  ADS_TRY(upload(lib->fstop, a->flat_frag_stop_idx, P, L, st));
-  if (lib->has_tol) ADS_TRY(upload(lib->ptol, a->precursor_rt_tolerance, P, L, st));
-  ADS_TRY(upload(lib->fmz, a->fragment_mz, NF, L, st));
-  ADS_TRY(upload(lib->fint, a->fragment_intensity, NF, L, st));
-  ADS_TRY(upload(lib->fnum, a->fragment_number, NF, L, st));
-  ADS_TRY(upload(lib->ftype, a->fragment_type, NF, L, st));
+  // one allocation for the library; a second, temporary one for the sort
+  auto plan_lib = [&](Carver& c) {
+    lib->pidx_p = c.take<uint64_t>(P);
+    lib->pmz_p = c.take<float>(P);
+    lib->prt_p = c.take<float>(P);
+    lib->ptol_p = lib->has_tol ? c.take<float>(P) : nullptr;
+    lib->fstart_p = c.take<uint64_t>(P);
+    lib->fstop_p = c.take<uint64_t>(P);
+    lib->fmz_p = c.take<float>(NF);
+    lib->fint_p = c.take<float>(NF);
+    lib->fnum_p = c.take<uint8_t>(NF);
+    lib->ftype_p = c.take<uint8_t>(NF);
+  };
+  Carver sizing;
+  plan_lib(sizing);
+  ADS_TRY(lib->arena.alloc(sizing.off));
+  Carver c{lib->arena.p, 0};
+  plan_lib(c);
 
-  if (P > 1) {
+  DevBuf<char> tmp;
+  Carver t;
+  uint64_t* pidx_in = nullptr;
+  float *pmz_in = nullptr, *prt_in = nullptr, *ptol_in = nullptr;
+  uint64_t *fs_in = nullptr, *fe_in = nullptr;
+  uint32_t *pos_in = nullptr, *pos_out = nullptr;
+  void* sort_tmp = nullptr;
+  size_t sort_bytes = 0;
+  const bool sort = P > 1;
+  if (sort) {
+    ADS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint64_t*)nullptr,
+                                             (uint64_t*)nullptr, (uint32_t*)nullptr,
+                                             (uint32_t*)nullptr, P, 0, 64, st));
+    auto plan_tmp = [&](Carver& q) {
+      pidx_in = q.take<uint64_t>(P);
+      pmz_in = q.take<float>(P);
+      prt_in = q.take<float>(P);
+      ptol_in = lib->has_tol ? q.take<float>(P) : nullptr;
+      fs_in = q.take<uint64_t>(P);
+      fe_in = q.take<uint64_t>(P);
+      pos_in = q.take<uint32_t>(P);
+      pos_out = q.take<uint32_t>(P);
+      sort_tmp = q.take<char>((int64_t)sort_bytes);
+    };
+    Carver tsize;
+    plan_tmp(tsize);
+    ADS_TRY(tmp.alloc(tsize.off));
+    t.base = tmp.p;
+    plan_tmp(t);
+  }
+  // precursor arrays land in the temporary area when they still need sorting
+  ADS_TRY(copy_in(sort ? pidx_in : lib->pidx_p, a->precursor_idx, P, L, st));
+  ADS_TRY(copy_in(sort ? pmz_in : lib->pmz_p, a->precursor_mz, P, L, st));
+  ADS_TRY(copy_in(sort ? prt_in : lib->prt_p, a->precursor_rt, P, L, st));
+  ADS_TRY(copy_in(sort ? fs_in : lib->fstart_p, a->flat_frag_start_idx, P, L, st));
+  ADS_TRY(copy_in(sort ? fe_in : lib->fstop_p, a->flat_frag_stop_idx, P, L, st));
+  if (lib->has_tol) ADS_TRY(copy_in(sort ? ptol_in : lib->ptol_p, a->precursor_rt_tolerance, P, L, st));
+  ADS_TRY(copy_in(lib->fmz_p, a->fragment_mz, NF, L, st));
+  ADS_TRY(copy_in(lib->fint_p, a->fragment_intensity, NF, L, st));
+  ADS_TRY(copy_in(lib->fnum_p, a->fragment_number, NF, L, st));
+  ADS_TRY(copy_in(lib->ftype_p, a->fragment_type, NF, L, st));
+
+  if (sort) {
     // stable radix sort of (precursor_idx, position): equal keys keep input order
-    DevBuf<uint64_t> keys_out;
-    DevBuf<uint32_t> pos_in, pos_out;
-    ADS_TRY(keys_out.alloc(P));
-    ADS_TRY(pos_in.alloc(P));
-    ADS_TRY(pos_out.alloc(P));
-    std::vector<uint32_t> iota((size_t)P);
-    for (int64_t i = 0; i < P; ++i) iota[i] = (uint32_t)i;
-    ADS_CUDA(cudaMemcpyAsync(pos_in.p, iota.data(), P * 4, cudaMemcpyHostToDevice, st));
-    size_t tb = 0;
-    ADS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, lib->pidx.p, keys_out.p, pos_in.p,
-                                             pos_out.p, P, 0, 64, st));
-    DevBuf<unsigned char> tmp;
-    ADS_TRY(tmp.alloc(tb + 16));
-    ADS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, lib->pidx.p, keys_out.p, pos_in.p,
-                                             pos_out.p, P, 0, 64, st));
-    ADS_CUDA(cudaStreamSynchronize(st));
-    lib->pidx = std::move(keys_out);
-    ADS_TRY(permute(lib->pmz, pos_out.p, P, st));
-    ADS_TRY(permute(lib->prt, pos_out.p, P, st));
-    ADS_TRY(permute(lib->fstart, pos_out.p, P, st));
-    ADS_TRY(permute(lib->fstop, pos_out.p, P, st));
-    if (lib->has_tol) ADS_TRY(permute(lib->ptol, pos_out.p, P, st));
+    iota_kernel<<<(int)std::min<int64_t>((P + 255) / 256, 4096), 256, 0, st>>>(P, pos_in);
+    ADS_LAUNCH_CHECK();
+    ADS_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, pidx_in, lib->pidx_p, pos_in,
+                                             pos_out, P, 0, 64, st));
+    launch_gather(P, pos_out, pmz_in, lib->pmz_p, st);
+    launch_gather(P, pos_out, prt_in, lib->prt_p, st);
+    launch_gather(P, pos_out, fs_in, lib->fstart_p, st);
+    launch_gather(P, pos_out, fe_in, lib->fstop_p, st);
+    if (lib->has_tol) launch_gather(P, pos_out, ptol_in, lib->ptol_p, st);
+    ADS_LAUNCH_CHECK();
   }
   ADS_CUDA(cudaStreamSynchronize(st));
   *out = lib.release();

@@ -420,19 +420,24 @@ struct AdsSelection {
 // that event from the collection's own copy stream.
 struct AdsCandidates {
   int device = 0;
-  cudaStream_t copy_stream = nullptr;
   cudaEvent_t done = nullptr;
-  int64_t cap = 0;
-  ads::DevBuf<uint64_t> pidx, rank, center, start, stop;
-  ads::DevBuf<float> score;
-  ads::DevBuf<int64_t> count_dev;
-  ads::DevBuf<int> err_dev;
+  int64_t cap = -1;
+  ads::DevBuf<char> arena;  // all columns and counters in one allocation
+  uint64_t* pidx_p = nullptr;
+  uint64_t* rank_p = nullptr;
+  uint64_t* center_p = nullptr;
+  uint64_t* start_p = nullptr;
+  uint64_t* stop_p = nullptr;
+  float* score_p = nullptr;
+  int64_t* count_p = nullptr;
+  int* err_p = nullptr;
   int64_t count = 0;
   bool pending = false;
   ~AdsCandidates() {
-    if (done) cudaEventSynchronize(done);
-    if (copy_stream) cudaStreamDestroy(copy_stream);
-    if (done) cudaEventDestroy(done);
+    if (done) {
+      cudaEventSynchronize(done);
+      cudaEventDestroy(done);
+    }
   }
 };
 
@@ -472,14 +477,19 @@ int64_t max_cycle_span(const std::vector<float>& rt, float delta_t, float tol, i
 }
 
 int reserve_candidates(AdsCandidates* c, int64_t cap) {
-  if (c->cap >= cap && c->pidx.p) return ADS_OK;
+  if (c->cap >= cap) return ADS_OK;
   const size_t n = (size_t)std::max<int64_t>(cap, 1);
-  ADS_TRY(c->pidx.alloc(n));
-  ADS_TRY(c->rank.alloc(n));
-  ADS_TRY(c->score.alloc(n));
-  ADS_TRY(c->center.alloc(n));
-  ADS_TRY(c->start.alloc(n));
-  ADS_TRY(c->stop.alloc(n));
+  const size_t col8 = (n * 8 + 255) / 256 * 256, col4 = (n * 4 + 255) / 256 * 256;
+  ADS_TRY(c->arena.alloc(5 * col8 + col4 + 256));
+  char* q = c->arena.p;
+  c->pidx_p = reinterpret_cast<uint64_t*>(q);
+  c->rank_p = reinterpret_cast<uint64_t*>(q + col8);
+  c->center_p = reinterpret_cast<uint64_t*>(q + 2 * col8);
+  c->start_p = reinterpret_cast<uint64_t*>(q + 3 * col8);
+  c->stop_p = reinterpret_cast<uint64_t*>(q + 4 * col8);
+  c->score_p = reinterpret_cast<float*>(q + 5 * col8);
+  c->count_p = reinterpret_cast<int64_t*>(q + 5 * col8 + col4);
+  c->err_p = reinterpret_cast<int*>(q + 5 * col8 + col4 + 8);
   c->cap = cap;
   return ADS_OK;
 }
@@ -489,10 +499,13 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
     return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
   DeviceGuard dg(s->device);
   cudaStream_t st = s->o.stream ? (cudaStream_t)s->o.stream : s->stream;
-  if (!c->done) ADS_CUDA(cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming));
-  if (!c->copy_stream) ADS_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-  // the previous read-out of these buffers must be complete before they are rewritten
-  ADS_CUDA(cudaStreamSynchronize(c->copy_stream));
+  if (!c->done) {
+    ADS_CUDA(cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming));
+  } else {
+    // a previous search into these buffers (possibly on another stream) comes first;
+    // read-outs are synchronous, so none is in flight
+    ADS_CUDA(cudaStreamWaitEvent(st, c->done, 0));
+  }
   const int64_t P = l->n_prec;
   const AdsSelectionParams& prm = s->p;
   const int L = (int)s->kernel.size();
@@ -509,11 +522,9 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   const int kf = (int)std::max<int64_t>(1, std::min<int64_t>(prm.top_k_fragments, l->max_frag));
   const int maxw = std::max(1, d->max_overlap);
 
-  ADS_TRY(c->count_dev.reserve(1));
-  ADS_TRY(c->err_dev.reserve(1));
   ADS_TRY(reserve_candidates(c, P * (int64_t)k_out));
-  ADS_CUDA(cudaMemsetAsync(c->count_dev.p, 0, sizeof(int64_t), st));
-  ADS_CUDA(cudaMemsetAsync(c->err_dev.p, 0, sizeof(int), st));
+  ADS_CUDA(cudaMemsetAsync(c->count_p, 0, sizeof(int64_t), st));
+  ADS_CUDA(cudaMemsetAsync(c->err_p, 0, sizeof(int), st));
   c->pending = true;
   c->count = 0;
   if (P == 0 || k_out == 0) {
@@ -551,16 +562,16 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
 
   PrepArgs pa;
   pa.n_prec = P;
-  pa.pmz = l->pmz.p;
-  pa.prt = l->prt.p;
-  pa.ptol = l->has_tol ? l->ptol.p : nullptr;
+  pa.pmz = l->pmz_p;
+  pa.prt = l->prt_p;
+  pa.ptol = l->has_tol ? l->ptol_p : nullptr;
   pa.rt_tol = prm.rt_tolerance;
-  pa.fstart = l->fstart.p;
-  pa.fstop = l->fstop.p;
-  pa.fmz = l->fmz.p;
-  pa.fint = l->fint.p;
-  pa.fnum = l->fnum.p;
-  pa.ftype = l->ftype.p;
+  pa.fstart = l->fstart_p;
+  pa.fstop = l->fstop_p;
+  pa.fmz = l->fmz_p;
+  pa.fint = l->fint_p;
+  pa.fnum = l->fnum_p;
+  pa.ftype = l->ftype_p;
   pa.rt = d->rt_dev.p;
   pa.n_rt = (int)n_rt;
   pa.delta_t = d->delta_t;
@@ -583,7 +594,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   pa.fw = s->fw.p;
   pa.blo = s->blo.p;
   pa.bhi = s->bhi.p;
-  pa.err = c->err_dev.p;
+  pa.err = c->err_p;
   ADS_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned int), st));
   const bool timed = s->o.time_stages != 0 && s->stage_used < 65536;
   if (timed) {
@@ -659,7 +670,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   sa.gather_mode = s->o.gather_mode;
   sa.scan_thresh = 4 * 32 * kPrefetchChunks;
   sa.work = s->work.p;
-  sa.err = c->err_dev.p;
+  sa.err = c->err_p;
   sa.cand_n = s->cand_n.p;
   sa.cand_score = s->cand_score.p;
   sa.cand_center = s->cand_center.p;
@@ -675,7 +686,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
 
   block_sum_kernel<<<(int)nb, kScanBlock, 0, st>>>(s->cand_n.p, P, s->block_sums.p);
   ADS_LAUNCH_CHECK();
-  scan_block_sums_kernel<<<1, kScanBlock, 0, st>>>(s->block_sums.p, nb, c->count_dev.p);
+  scan_block_sums_kernel<<<1, kScanBlock, 0, st>>>(s->block_sums.p, nb, c->count_p);
   ADS_LAUNCH_CHECK();
   ScatterArgs ca;
   ca.n_prec = P;
@@ -685,14 +696,14 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   ca.cand_n = s->cand_n.p;
   ca.cand_score = s->cand_score.p;
   ca.cand_center = s->cand_center.p;
-  ca.pidx = l->pidx.p;
+  ca.pidx = l->pidx_p;
   ca.block_off = s->block_sums.p;
-  ca.o_pidx = c->pidx.p;
-  ca.o_rank = c->rank.p;
-  ca.o_score = c->score.p;
-  ca.o_center = c->center.p;
-  ca.o_start = c->start.p;
-  ca.o_stop = c->stop.p;
+  ca.o_pidx = c->pidx_p;
+  ca.o_rank = c->rank_p;
+  ca.o_score = c->score_p;
+  ca.o_center = c->center_p;
+  ca.o_start = c->start_p;
+  ca.o_stop = c->stop_p;
   scatter_kernel<<<(int)nb, kScanBlock, 0, st>>>(ca);
   ADS_LAUNCH_CHECK();
   launches += 3;
@@ -710,11 +721,11 @@ int finish(AdsCandidates* c) {
   DeviceGuard dg(c->device);
   int64_t cnt = 0;
   int err = 0;
-  ADS_CUDA(cudaStreamWaitEvent(c->copy_stream, c->done, 0));
-  ADS_CUDA(cudaMemcpyAsync(&cnt, c->count_dev.p, sizeof(int64_t), cudaMemcpyDeviceToHost,
-                           c->copy_stream));
-  ADS_CUDA(cudaMemcpyAsync(&err, c->err_dev.p, sizeof(int), cudaMemcpyDeviceToHost, c->copy_stream));
-  ADS_CUDA(cudaStreamSynchronize(c->copy_stream));
+  ADS_CUDA(cudaStreamWaitEvent(cudaStreamPerThread, c->done, 0));
+  ADS_CUDA(cudaMemcpyAsync(&cnt, c->count_p, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                           cudaStreamPerThread));
+  ADS_CUDA(cudaMemcpyAsync(&err, c->err_p, sizeof(int), cudaMemcpyDeviceToHost, cudaStreamPerThread));
+  ADS_CUDA(cudaStreamSynchronize(cudaStreamPerThread));
   c->pending = false;
   if (err)
     return fail(ADS_ERR_INTERNAL, "search kernel reported internal error flags " + std::to_string(err));
@@ -930,15 +941,15 @@ int ads_candidates_copy_out(AdsCandidates* c, uint64_t* pidx, uint64_t* rank, fl
       void* dst;
       const void* src;
       size_t bytes;
-    } cols[] = {{pidx, c->pidx.p, 8}, {rank, c->rank.p, 8},   {score, c->score.p, 4},
-                {center, c->center.p, 8}, {start, c->start.p, 8}, {stop, c->stop.p, 8}};
+    } cols[] = {{pidx, c->pidx_p, 8}, {rank, c->rank_p, 8},   {score, c->score_p, 4},
+                {center, c->center_p, 8}, {start, c->start_p, 8}, {stop, c->stop_p, 8}};
     for (auto& col : cols)
       if (col.dst)
         ADS_CUDA(cudaMemcpyAsync(col.dst, col.src, n * col.bytes, cudaMemcpyDeviceToHost,
-                                 c->copy_stream));
+                                 cudaStreamPerThread));
     for (uint64_t* z : {scan_center, scan_start, scan_stop})
       if (z) std::memset(z, 0, n * 8);
-    ADS_CUDA(cudaStreamSynchronize(c->copy_stream));
+    ADS_CUDA(cudaStreamSynchronize(cudaStreamPerThread));
     return ADS_OK;
   });
 }
