@@ -95,6 +95,7 @@ class AdsEngineOptions(C.Structure):
         ("blocks_per_sm", i32),
         ("gather_mode", i32),
         ("time_stages", i32),
+        ("cycles_per_lane", i32),
         ("stream", i64),
     ]
 

@@ -23,6 +23,20 @@ def _lib():
     return F.load()
 
 
+def _release(obj, destroy: str) -> None:
+    """Frees a native handle from __del__; silent during interpreter shutdown, when
+    module globals may already be gone."""
+    h = getattr(obj, "_h", None)
+    obj._h = None
+    if not h:
+        return
+    try:
+        if F.alive():
+            getattr(_lib(), destroy)(h)
+    except Exception:
+        pass
+
+
 def _is_device_tensor(x: Any) -> bool:
     return hasattr(x, "is_cuda") and bool(getattr(x, "is_cuda"))
 
@@ -64,13 +78,7 @@ class DIAData:
         self.device = _DEFAULT_DEVICE
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h and F.alive():
-            try:
-                _lib().ads_dia_destroy(h)
-            except Exception:
-                pass
-            self._h = None
+        _release(self, "ads_dia_destroy")
 
     @staticmethod
     def from_arrays(spectrum_delta_scan_idx, isolation_lower_mz, isolation_upper_mz,
@@ -220,13 +228,7 @@ class SpecLibFlat:
         self.device = _DEFAULT_DEVICE
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h and F.alive():
-            try:
-                _lib().ads_lib_destroy(h)
-            except Exception:
-                pass
-            self._h = None
+        _release(self, "ads_lib_destroy")
 
     @staticmethod
     def from_arrays(precursor_idx, precursor_mz_library, precursor_mz, precursor_rt_library,
@@ -368,13 +370,7 @@ class CandidateCollection:
         self._n = 0
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h and F.alive():
-            try:
-                _lib().ads_candidates_destroy(h)
-            except Exception:
-                pass
-            self._h = None
+        _release(self, "ads_candidates_destroy")
 
     @classmethod
     def _from_handle(cls, h: int) -> "CandidateCollection":
@@ -453,7 +449,8 @@ class PeakGroupSelection:
 
     def __init__(self, params: SelectionParameters, *, precision: str = "fp32", verbose: bool = True,
                  device: int | None = None, warps_per_block: int = 0, blocks_per_sm: int = 0,
-                 gather_mode: int = 0, time_stages: bool = False, stream: int = 0):
+                 gather_mode: int = 0, time_stages: bool = False, stream: int = 0,
+                 cycles_per_lane: int = 0):
         if not isinstance(params, SelectionParameters):
             raise TypeError("argument 'params': expected SelectionParameters")
         L = _lib()
@@ -467,6 +464,7 @@ class PeakGroupSelection:
         o.blocks_per_sm = blocks_per_sm
         o.gather_mode = gather_mode
         o.time_stages = 1 if time_stages else 0
+        o.cycles_per_lane = int(cycles_per_lane)
         o.stream = int(stream)
         self._opts = o
         p = params._c()
@@ -475,13 +473,7 @@ class PeakGroupSelection:
         self._h = h.value
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h and F.alive():
-            try:
-                _lib().ads_selection_destroy(h)
-            except Exception:
-                pass
-            self._h = None
+        _release(self, "ads_selection_destroy")
 
     def search(self, dia_data: DIAData, lib: SpecLibFlat) -> CandidateCollection:
         if not isinstance(dia_data, DIAData) or not isinstance(lib, SpecLibFlat):
@@ -543,13 +535,7 @@ class DeviceCandidates:
         self._h = h.value
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h and F.alive():
-            try:
-                _lib().ads_candidates_destroy(h)
-            except Exception:
-                pass
-            self._h = None
+        _release(self, "ads_candidates_destroy")
 
     def size(self) -> int:
         n = int(_lib().ads_candidates_size(self._h))

@@ -111,6 +111,16 @@ std::mutex g_ln_mu;
 std::map<int, double2*> g_ln_tables;
 }  // namespace
 
+std::vector<double2> host_ln_table() {
+  std::vector<double2> tab(kLnTableSize);
+  for (int j = 0; j < kLnTableSize; ++j) {
+    const double c = 1.0 + (double)j / kLnTableSize;
+    tab[j].x = 1.0 / c;
+    tab[j].y = std::log(c);
+  }
+  return tab;
+}
+
 int device_ln_table(int device, const double2** out) {
   std::lock_guard<std::mutex> lk(g_ln_mu);
   auto it = g_ln_tables.find(device);
@@ -118,12 +128,7 @@ int device_ln_table(int device, const double2** out) {
     *out = it->second;
     return ADS_OK;
   }
-  std::vector<double2> tab(kLnTableSize);
-  for (int j = 0; j < kLnTableSize; ++j) {
-    const double c = 1.0 + (double)j / kLnTableSize;
-    tab[j].x = 1.0 / c;
-    tab[j].y = std::log(c);
-  }
+  const std::vector<double2> tab = host_ln_table();
   DeviceGuard dg(device);
   double2* d = nullptr;
   ADS_CUDA(cudaMalloc(&d, kLnTableSize * sizeof(double2)));

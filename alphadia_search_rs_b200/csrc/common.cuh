@@ -195,13 +195,16 @@ static __device__ __noinline__ float ln_rn_slow(float x) {
 constexpr int kLnTableBits = 8;
 constexpr int kLnTableSize = 1 << kLnTableBits;
 int device_ln_table(int device, const double2** out);
+std::vector<double2> host_ln_table();  // the values device_ln_table uploads
 
 // The same value as ln_rn(x) for every float x, computed faster: x = 2^e * m,
-// m = c_j * (1 + r) with |r| < 2^-8, ln(1 + r) by its Taylor series to r^7, all in
-// double (error below 2^-40 relative).  If the double result lies within a
-// generous margin (2^-38 relative) of a float rounding boundary -- about one input
-// in 2^14 -- ln_rn decides; elsewhere both round to the same float.  `tab` is the
-// table of device_ln_table (usually staged in shared memory).
+// m = c_j * (1 + r) with 0 <= r < 2^-8, ln(1 + r) by its Taylor series to r^5,
+// all in double; every term is non-negative for x > 1, so the result y carries a
+// relative error below 2^-42.  Rounding y to float is then correct unless the 29
+// bits of y's significand below float precision lie within 2^14 units of the
+// halfway pattern (about one input in 2^14); there ln_rn decides.  Checked against
+// ln_rn for every float in (1, inf).  `tab` is the table of device_ln_table
+// (usually staged in shared memory).
 __device__ __forceinline__ float ln_fast(float x, const double2* tab, bool* slow = nullptr) {
   const uint32_t b = __float_as_uint(x);
   if (b <= 0x3F800000u || b >= 0x7F800000u) {  // x <= 1, negative, inf or NaN
@@ -212,28 +215,19 @@ __device__ __forceinline__ float ln_fast(float x, const double2* tab, bool* slow
   const double m = (double)__uint_as_float((b & 0x007FFFFFu) | 0x3F800000u);
   const double2 t = tab[j];
   const double r = fma(m, t.x, -1.0);
-  double p = 1.0 / 7.0;
-  p = fma(p, r, -1.0 / 6.0);
-  p = fma(p, r, 1.0 / 5.0);
+  double p = 1.0 / 5.0;
   p = fma(p, r, -1.0 / 4.0);
   p = fma(p, r, 1.0 / 3.0);
   p = fma(p, r, -1.0 / 2.0);
   p = fma(p, r, 1.0);
-  p = p * r;
   const double ln2 = 0.6931471805599453094172321;
-  const double y = fma((double)e, ln2, t.y + p);
-  const float f = __double2float_rn(y);
-  const uint32_t fb = __float_as_uint(f);  // f is a positive normal float
-  const uint32_t fe = (fb >> 23) & 0xFFu;
-  double half_ulp = __longlong_as_double((long long)(fe - 127 - 24 + 1023) << 52);
-  // below a power of two the spacing (and the distance to the boundary) halves
-  if ((fb & 0x007FFFFFu) == 0 && y < (double)f) half_ulp *= 0.5;
-  const double dist = fabs(y - (double)f);
-  if (half_ulp - dist <= y * 0x1p-38) {
+  const double y = fma((double)e, ln2, fma(p, r, t.y));
+  const uint32_t low = (uint32_t)__double2loint(y) & 0x1FFFFFFFu;
+  if (low - (0x10000000u - 0x4000u) < 0x8000u) {
     if (slow) *slow = true;
     return ln_rn_slow(x);
   }
-  return f;
+  return __double2float_rn(y);
 }
 
 // ------------------------------------------------------------- structures

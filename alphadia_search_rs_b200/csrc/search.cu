@@ -290,6 +290,31 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a) {
 
 #include "search_kernel.cuh"
 
+// Cycles per lane the search kernel is compiled for, and its instances: fully
+// unrolled stencils for the half widths of kernel_size 20, 21-22 and 31-32, any
+// other half width through the generic path.
+constexpr int kLaneCycles[] = {4, 8, 10, 13, 16};
+
+template <int H>
+void (*pick_for_h(int S))(SearchArgs) {
+  switch (S) {
+    case 4: return search_kernel<H, 4>;
+    case 8: return search_kernel<H, 8>;
+    case 10: return search_kernel<H, 10>;
+    case 13: return search_kernel<H, 13>;
+    default: return search_kernel<H, 16>;
+  }
+}
+
+void (*pick_search_kernel(int h, int S))(SearchArgs) {
+  switch (h) {
+    case 10: return pick_for_h<10>(S);
+    case 11: return pick_for_h<11>(S);
+    case 16: return pick_for_h<16>(S);
+    default: return pick_for_h<0>(S);
+  }
+}
+
 // ------------------------------------------------------------ compaction
 
 __device__ __forceinline__ int64_t block_exclusive_scan(int64_t v, int64_t* sh, int64_t* total) {
@@ -406,7 +431,7 @@ struct AdsSelection {
   ads::DevBuf<float> fw, cand_score;
   ads::DevBuf<uint32_t> blo, bhi;
   ads::DevBuf<uint8_t> keep;
-  ads::DevBuf<unsigned int> work;
+  ads::DevBuf<unsigned long long> work;
   ads::DevBuf<int64_t> block_sums;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // one set of four events per timed search since the last read-out
@@ -514,11 +539,26 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
 
   const float tol_max = l->has_tol ? std::max(l->max_tol, 0.0f) : prm.rt_tolerance;
   const int64_t c_max = std::max<int64_t>(1, max_cycle_span(d->rt, d->delta_t, tol_max, prm.kernel_size));
-  const int cp = (int)((c_max + 31) / 32 * 32);
-  if (cp > (1 << kListRowShift))
+  if (c_max > kMaxCycles)
     return fail(ADS_ERR_INVALID_ARGUMENT, "RT windows longer than 2048 cycles are not supported (" +
                                               std::to_string(c_max) + " cycles)");
-  const int k_out = (int)std::max<int64_t>(0, std::min<int64_t>(prm.candidate_count, maxima_cap(cp)));
+  // cycles per lane: the fewest lane slots (passes * 32 * S) covering c_max, ties to
+  // the larger S
+  int S = s->o.cycles_per_lane;
+  if (S == 0) {
+    int64_t best = -1;
+    for (int cand : kLaneCycles) {
+      const int64_t slots = (c_max + 32 * cand - 1) / (32 * cand) * 32 * cand;
+      if (best < 0 || slots <= best) {
+        best = slots;
+        S = cand;
+      }
+    }
+  }
+  if (std::find(std::begin(kLaneCycles), std::end(kLaneCycles), S) == std::end(kLaneCycles))
+    return fail(ADS_ERR_INVALID_ARGUMENT, "cycles_per_lane must be 0 or one of 4, 8, 10, 13, 16");
+  const int ncell = (int)((c_max + 32 * S - 1) / (32 * S) * 32 * S);
+  const int k_out = (int)std::max<int64_t>(0, std::min<int64_t>(prm.candidate_count, maxima_cap(ncell)));
   const int kf = (int)std::max<int64_t>(1, std::min<int64_t>(prm.top_k_fragments, l->max_frag));
   const int maxw = std::max(1, d->max_overlap);
 
@@ -595,7 +635,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   pa.blo = s->blo.p;
   pa.bhi = s->bhi.p;
   pa.err = c->err_p;
-  ADS_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned int), st));
+  ADS_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned long long), st));
   const bool timed = s->o.time_stages != 0 && s->stage_used < 65536;
   if (timed) {
     if (s->stage_used == s->stage_pool.size()) {
@@ -612,31 +652,19 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
     ++launches;
   }
 
-  // block shape: warps per block (option or default) and how many fragment rows
-  // of the XIC fit in shared memory at once
-  int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : 4;
+  // block shape: warps per block (one precursor per warp at a time)
+  int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : 8;
   nw = std::max(1, std::min(nw, 8));
   int max_smem = 0;
   ADS_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
-  const size_t budget = std::min<size_t>((size_t)max_smem, 96 * 1024);
-  int rows = kf;
-  auto plan_bytes = [&](int w, int r) { return (size_t)smem_plan(w, cp, r).total * 4; };
-  while (rows > 1 && plan_bytes(nw, rows) > budget) --rows;
-  while (nw > 1 && plan_bytes(nw, rows) > (size_t)max_smem) --nw;
-  const size_t smem = plan_bytes(nw, rows);
+  while (nw > 1 && search_smem_bytes(nw, S, s->h, ncell) > (size_t)max_smem) --nw;
+  const size_t smem = search_smem_bytes(nw, S, s->h, ncell);
   if (smem > (size_t)max_smem)
     return fail(ADS_ERR_INVALID_ARGUMENT, "RT window too long for shared memory (" +
                                               std::to_string(c_max) + " cycles)");
   const double2* ln_tab = nullptr;
   ADS_TRY(device_ln_table(s->device, &ln_tab));
-  void (*kern)(SearchArgs);
-  switch (s->h) {
-    case 10: kern = search_kernel<10>; break;
-    case 11: kern = search_kernel<11>; break;
-    case 15: kern = search_kernel<15>; break;
-    case 16: kern = search_kernel<16>; break;
-    default: kern = search_kernel<0>; break;
-  }
+  void (*kern)(SearchArgs) = pick_search_kernel(s->h, S);
   ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
@@ -665,8 +693,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   sa.h = s->h;
   sa.k_out = k_out;
   sa.c_max = (int)c_max;
-  sa.cp = cp;
-  sa.rows = rows;
+  sa.ncell = ncell;
   sa.gather_mode = s->o.gather_mode;
   sa.scan_thresh = 4 * 32 * kPrefetchChunks;
   sa.work = s->work.p;
@@ -677,7 +704,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   sa.stats = s->stats_on ? s->stats.p : nullptr;
   if (timed) ADS_CUDA(cudaEventRecord(s->stage_ev[1], st));
   {
-    const int64_t blocks = std::min<int64_t>((int64_t)s->num_sms * bps, P);
+    const int64_t blocks = std::min<int64_t>((int64_t)s->num_sms * bps, (P + nw - 1) / nw);
     kern<<<(int)blocks, nw * 32, smem, st>>>(sa);
     ADS_LAUNCH_CHECK();
     ++launches;

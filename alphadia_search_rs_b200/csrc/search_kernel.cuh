@@ -3,22 +3,20 @@
 // Included by search.cu inside namespace ads::{anonymous}; uses its helpers
 // (kFull, rust_bsearch_u16, lower_bound_u16).
 //
-// Per precursor (one block, persistent over an atomic work counter), in rounds of
-// `rows` fragments (one round when the whole XIC fits in shared memory):
-//   1. gather   warps take fragments round-robin; per (fragment, window) the CSR
-//               offsets of all the warp's pairs are fetched together, then up to
-//               128 entries of a bin range are read in one round trip and added to
-//               the fragment's XIC row in CSR order;
-//   2. list     the outputs whose 2h+1 input window holds a nonzero cell (the
-//               bitmap of touched cells dilated by h, inside the valid region) are
-//               collected into a list; every other output is exactly zero;
-//   3. convolve every thread takes list entries: single-input windows take one
-//               multiply, the others run the reference's stencil (fully unrolled
-//               for the common half widths);
-//   4. score    score[j] += ln(conv_f[j] + 1) * w_f in fragment order (logs only
-//               for nonzero values);
-// then maxima and top-K.  All f32 arithmetic is explicitly rounded and in the
-// reference's order, so results equal the reference's except for its logf.
+// One warp per precursor; warps pull precursors from an atomic counter and never
+// wait on each other after the block has staged its tables.  The warp walks the
+// precursor's kept fragments in order and, for each one,
+//   1. gathers the fragment's XIC row into its shared-memory row: the CSR
+//      entries of every (fragment, window) pair are read up to 128 at a time and
+//      added to the row in CSR order (the reference's `dense_xic[c] += intensity`);
+//   2. convolves the row: lane l owns S consecutive output cycles per pass of
+//      32*S cycles and holds the S + 2h inputs they need in registers;
+//   3. adds ln(conv + 1) * w_f to its own columns' scores.  Fragments are taken
+//      in order, which is the reference's row-major accumulation
+//      (src/score/scalar.rs:16-22).
+// Then 5-point local maxima over the scores and a warp top-K.  All f32
+// arithmetic is explicitly rounded and in the reference's order, so results
+// equal the reference's except for its logf (see ln_rn).
 
 struct SearchArgs {
   int64_t n_prec;
@@ -41,11 +39,10 @@ struct SearchArgs {
   int h;
   int k_out;   // candidates kept per precursor
   int c_max;   // largest cycle range any precursor can have
-  int cp;      // c_max rounded up to 32
-  int rows;    // XIC rows held in shared memory (fragments per round)
+  int ncell;   // cycles a warp's row holds: passes * 32 * S >= c_max
   int gather_mode;
   int scan_thresh;
-  unsigned int* work;
+  unsigned long long* work;
   int* err;
   int* cand_n;
   float* cand_score;
@@ -54,53 +51,64 @@ struct SearchArgs {
 };
 
 constexpr int kPrefetchChunks = 4;  // 4 x 32 CSR entries read per round trip
-constexpr int kListRowShift = 11;   // list entry = row << 11 | cycle (cycle < 2048)
+constexpr int kBitOff = 32;         // bitmap bit of cycle c is c + kBitOff (room for -h)
+constexpr int kMaxCycles = 2048;    // longest RT window (cycles) a precursor may span
 
-// XIC rows are stored skewed, cycle j at j + j/8, so that reads of neighbouring
-// cycles by neighbouring threads spread over the shared-memory banks.
-__host__ __device__ __forceinline__ int xs(int j) { return j + (j >> 3); }
-__host__ __device__ __forceinline__ int row_stride(int cp) { return cp + cp / 8; }
+__host__ __device__ inline int maxima_cap(int ncell) { return ncell / 4 + 8; }
 
-__host__ __device__ inline int bitmap_words(int cp) { return cp / 32 + 3; }
-__host__ __device__ inline int maxima_cap(int cp) { return cp / 4 + 8; }
+// Shared-memory address of stored index i (cycle + off) in a row or score array
+// whose lanes own S consecutive cycles: one pad word after every S cells, so that
+// the 32 lanes of a warp, reading at the same offset within their segments, hit
+// 32 different banks.
+template <int S>
+__device__ __forceinline__ int xaddr(int i) {
+  return i + i / S;
+}
 
-// Shared-memory plan, in 4-byte words.  The per-warp duplicate tags of the gather
-// and the convolved rows of the later phases share one region.
-struct SmemPlan {
-  int ln, kw, xrow, vrow, tags, list, bm, scr, score, mval, midx, misc, total;
-  int bw, mx;
+// Floor division, for offsets known at compile time.
+__host__ __device__ constexpr int floordiv(int a, int b) {
+  return a >= 0 ? a / b : -((-a + b - 1) / b);
+}
+
+// Per-warp shared-memory plan, in 4-byte words.  The block's ln table (double2 x
+// 256 = 1024 words) and kernel taps (32 words) come first.
+struct WarpPlan {
+  int row, tags, bm, scr, score, mval, midx, total;
+  int off;        // stored index of cycle c is c + off (off >= h, a multiple of S)
+  int row_words;  // words of the row, a multiple of 4
+  int bw;         // bitmap words
+  int mx;         // maxima capacity
 };
+constexpr int kBlockHeaderWords = kLnTableSize * 4 + 32;
 
-__host__ __device__ inline SmemPlan smem_plan(int nw, int cp, int rows) {
-  SmemPlan s;
+__host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
+  WarpPlan w;
+  w.off = (h + S - 1) / S * S;
+  const int span = ncell + h + w.off + S;  // stored indices [0, span) cover every read
+  w.row_words = (span + span / S + 1 + 3) & ~3;
   int o = 0;
-  s.bw = bitmap_words(cp);
-  s.mx = maxima_cap(cp);
-  s.ln = o;
-  o += kLnTableSize * 4;
-  s.kw = o;
+  w.row = o;
+  o += w.row_words;
+  w.tags = o;
+  o += ncell;
+  w.bw = (ncell + 2 * kBitOff + 32) / 32 + 2;
+  w.bm = o;
+  o += w.bw;
+  w.scr = o;
   o += 32;
-  s.xrow = o;
-  o += rows * row_stride(cp);
-  s.vrow = o;
-  s.tags = o;
-  o += (rows > nw ? rows : nw) * cp;
-  s.list = o;
-  o += (rows * cp + 1) / 2;  // u16 entries
-  s.bm = o;
-  o += rows * s.bw;
-  s.scr = o;
-  o += nw * 32;
-  s.score = o;
-  o += cp;
-  s.mval = o;
-  o += s.mx;
-  s.midx = o;
-  o += s.mx;
-  s.misc = o;
-  o += 8;
-  s.total = o;
-  return s;
+  w.score = o + 4;  // 4 words of margin below: the maxima scan reads 2 cycles early
+  o += ncell + ncell / S + 12;
+  w.mx = maxima_cap(ncell);
+  w.mval = o;
+  o += w.mx;
+  w.midx = o;
+  o += w.mx;
+  w.total = (o + 3) & ~3;
+  return w;
+}
+
+__host__ __device__ inline size_t search_smem_bytes(int nw, int S, int h, int ncell) {
+  return (size_t)(kBlockHeaderWords + nw * warp_plan(S, h, ncell).total) * 4;
 }
 
 struct Counters {
@@ -109,11 +117,11 @@ struct Counters {
 
 // Adds one chunk of 32 CSR-consecutive entries to the XIC row in lane order (the
 // reference's `dense_xic[c] += intensity`, src/quadrupole_observation/mod.rs:96-105).
-// A tag per cell detects whether two accepted lanes hit the same cycle; only then
+// A tag per cycle detects whether two accepted lanes hit the same cycle; only then
 // are the lanes grouped and summed by their lowest lane one rounded add at a time.
-// The detection never misses a collision, whatever stale tags hold.
-__device__ __forceinline__ void add_chunk(bool inc, int cell, float v, int lane, float* row,
-                                          uint32_t* bm, uint32_t* tags, float* scr,
+// Tags only grow (seq), so stale tags from earlier chunks never hide a collision.
+__device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v, int lane,
+                                          float* row, uint32_t* bm, uint32_t* tags, float* scr,
                                           uint32_t& seq, unsigned long long& n_acc) {
   const unsigned act = __ballot_sync(kFull, inc);
   if (act == 0) return;
@@ -124,10 +132,11 @@ __device__ __forceinline__ void add_chunk(bool inc, int cell, float v, int lane,
   if (inc) old = atomicMax(tags + cell, mytag);
   __syncwarp();
   const bool dup = inc && (tags[cell] != mytag || (old >> 5) == (mytag >> 5));
+  const int bit = cell + kBitOff;
   if (!__any_sync(kFull, dup)) {
     if (inc) {
-      row[xs(cell)] = __fadd_rn(row[xs(cell)], v);
-      atomicOr(bm + (cell >> 5), 1u << (cell & 31));
+      row[addr] = __fadd_rn(row[addr], v);
+      atomicOr(bm + (bit >> 5), 1u << (bit & 31));
     }
   } else {
     const int key = inc ? cell : (-1 - lane);
@@ -135,15 +144,15 @@ __device__ __forceinline__ void add_chunk(bool inc, int cell, float v, int lane,
     scr[lane] = v;
     __syncwarp();
     if (inc && lane == __ffs(grp) - 1) {
-      float acc = row[xs(cell)];
+      float acc = row[addr];
       unsigned g = grp;
       while (g) {
         const int l = __ffs(g) - 1;
         acc = __fadd_rn(acc, scr[l]);
         g &= g - 1;
       }
-      row[xs(cell)] = acc;
-      atomicOr(bm + (cell >> 5), 1u << (cell & 31));
+      row[addr] = acc;
+      atomicOr(bm + (bit >> 5), 1u << (bit & 31));
     }
   }
   __syncwarp();
@@ -170,10 +179,10 @@ __device__ __forceinline__ bool bin_starts_at(const uint32_t* ssw, uint32_t b0, 
 //            lands, src/quadrupole_observation/mod.rs:91-94);
 //   bsearch  per bin, binary-search the first kept entry and the first entry at or
 //            past stop, then read only the kept entries.
+template <int S>
 __device__ void gather_pair(const SearchArgs& a, const WinInfo& wi, uint32_t b0, uint32_t b1,
-                            int64_t rs, int64_t re, int cs, int ce, int lane, float* row,
-                            uint32_t* bm, uint32_t* tags, float* scr, uint32_t& seq,
-                            Counters& k) {
+                            int64_t rs, int64_t re, int cs, int ce, int lane, float* row, int off,
+                            uint32_t* bm, uint32_t* tags, float* scr, uint32_t& seq, Counters& k) {
   const int64_t n = re - rs;
   if (n <= 0) return;
   const uint32_t* ssw = a.ss + wi.ss_off;
@@ -211,7 +220,9 @@ __device__ void gather_pair(const SearchArgs& a, const WinInfo& wi, uint32_t b0,
           }
           inc = last;
         }
-        add_chunk(inc, cu - cs, v[u], lane, row, bm, tags, scr, seq, k.acc);
+        const int cell = cu - cs;
+        add_chunk(inc, cell, inc ? xaddr<S>(cell + off) : 0, v[u], lane, row, bm, tags, scr, seq,
+                  k.acc);
       }
     }
   } else {
@@ -250,280 +261,275 @@ __device__ void gather_pair(const SearchArgs& a, const WinInfo& wi, uint32_t b0,
         const int64_t q = opos + (t - oex);
         const int c = vt ? (int)__ldg(cy + q) : 0;
         const float v = vt ? __ldg(in + q) : 0.0f;
-        add_chunk(vt, c - cs, v, lane, row, bm, tags, scr, seq, k.acc);
+        const int cell = c - cs;
+        add_chunk(vt, cell, vt ? xaddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, seq, k.acc);
       }
     }
   }
 }
 
-// nbits (<= 63) bitmap bits starting at bit p0 (p0 may be negative: bits below 0
-// are zero).
-__device__ __forceinline__ uint64_t window_bits(const uint32_t* bm, int p0, int nbits) {
-  int shift = 0;
-  if (p0 < 0) {
-    shift = -p0;
-    nbits -= shift;
-    p0 = 0;
-    if (nbits <= 0) return 0;
+// Any bit set in bm[lo, lo + n)?  (lo >= 0, n >= 1)
+__device__ __forceinline__ bool bits_any(const uint32_t* bm, int lo, int n) {
+  const int last = lo + n - 1;
+  const int w0 = lo >> 5, w1 = last >> 5;
+  uint32_t acc = 0;
+  for (int w = w0; w <= w1; ++w) {
+    uint32_t v = bm[w];
+    if (w == w0) v &= 0xffffffffu << (lo & 31);
+    if (w == w1) v &= 0xffffffffu >> (31 - (last & 31));
+    acc |= v;
   }
-  const int w = p0 >> 5, off = p0 & 31;
-  const uint64_t lo = (uint64_t)bm[w] | ((uint64_t)bm[w + 1] << 32);
-  uint64_t r = lo >> off;
-  if (off) r |= (uint64_t)bm[w + 2] << (64 - off);
-  r &= (1ull << nbits) - 1;
-  return r << shift;
+  return acc != 0u;
 }
 
-
-// Active outputs of one 32-cycle word of a row: the touched-cell bitmap dilated
-// by h (cycle j is active if a touched cell lies in [j - h, j + h]), limited to the
-// valid region [h, C - h) where the reference computes anything.
-__device__ __forceinline__ uint32_t active_word(const uint32_t* bm, int w, int h, int C) {
-  const uint32_t c = bm[w], p = w > 0 ? bm[w - 1] : 0u, n = bm[w + 1];
-  uint32_t act = c;
-  for (int d = 1; d <= h; ++d) act |= (c << d) | (p >> (32 - d)) | (c >> d) | (n << (32 - d));
-  const int j0 = w * 32;
-  const int lo = max(h - j0, 0), hi = min(C - h - j0, 32);  // valid bit range [lo, hi)
-  if (hi <= lo) return 0u;
-  const uint32_t upper = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
-  const uint32_t lower = (1u << lo) - 1u;
-  return act & upper & ~lower;
-}
-
-// One output of convolution_scalar (src/convolution/scalar.rs:30-50): x[j]*w[h]
-// first, then (x[j-d] + x[j+d]) * w[h-d] for d = h..1.  Inputs that are zero add
-// +0, so a window with a single nonzero input reduces to that input times its
-// tap, exactly.
-template <int H>
-__device__ __forceinline__ float conv_output(const SearchArgs& a, const float* x,
-                                             const uint32_t* bm, const float* kw_s, int j) {
-  const int h = H > 0 ? H : a.h;
-  const uint64_t m = window_bits(bm, j - h, 2 * h + 1);
-  if (__popcll(m) == 1) {
-    const int d = abs(__ffsll((long long)m) - 1 - h);
-    return __fmul_rn(x[xs(j - h + __ffsll((long long)m) - 1)], kw_s[h - d]);
-  }
-  if (H > 0) {
-    float s = __fadd_rn(0.0f, __fmul_rn(x[xs(j)], a.kw[H]));
-#pragma unroll
-    for (int k = 0; k < H; ++k)
-      s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[xs(j - H + k)], x[xs(j + H - k)]), a.kw[k]));
-    return s;
-  }
-  // any half width: only the nonzero tap pairs, in the reference order
-  float s = __fadd_rn(0.0f, __fmul_rn(x[xs(j)], kw_s[h]));
-  const uint32_t lmask = (1u << h) - 1u;
-  const uint32_t lb = (uint32_t)m & lmask;
-  const uint32_t rb = (uint32_t)(m >> (h + 1)) & lmask;
-  uint32_t D = lb | (__brev(rb) >> (32 - h));
-  while (D) {
-    const int k = __ffs(D) - 1;
-    const int d = h - k;
-    s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[xs(j - d)], x[xs(j + d)]), kw_s[k]));
-    D &= D - 1;
-  }
+// One output of convolution_scalar (src/convolution/scalar.rs:30-50) read from the
+// row in shared memory: x[j]*w[h] first, then (x[j-d] + x[j+d]) * w[h-d] for
+// d = h..1.  Any half width; used off the main path.
+template <int S>
+__device__ __forceinline__ float conv_at(const float* row, int off, const float* kw_s, int h,
+                                         int j) {
+  float s = __fadd_rn(0.0f, __fmul_rn(row[xaddr<S>(j + off)], kw_s[h]));
+  for (int t = 0; t < h; ++t)
+    s = __fadd_rn(s, __fmul_rn(__fadd_rn(row[xaddr<S>(j - h + t + off)], row[xaddr<S>(j + h - t + off)]),
+                              kw_s[t]));
   return s;
 }
 
-template <int H>
-__global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
+// score[j] += ln(c + 1) * w, one rounded operation at a time (src/score/scalar.rs:16-22).
+__device__ __forceinline__ void score_add(float* score, int addr, float c, float w,
+                                          const double2* lnt) {
+  score[addr] = __fadd_rn(score[addr], __fmul_rn(ln_fast(__fadd_rn(c, 1.0f), lnt), w));
+}
+
+template <int H, int S>
+__global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
   extern __shared__ __align__(16) float smem_raw[];
-  const int nw = blockDim.x >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const SmemPlan P = smem_plan(nw, a.cp, a.rows);
-  uint32_t* sw = reinterpret_cast<uint32_t*>(smem_raw);
-  double2* lnt = reinterpret_cast<double2*>(smem_raw + P.ln);
-  float* kw_s = smem_raw + P.kw;
-  float* xrow = smem_raw + P.xrow;
-  float* vrow = smem_raw + P.vrow;
-  uint32_t* tags = sw + P.tags + warp * a.cp;
-  uint16_t* list = reinterpret_cast<uint16_t*>(sw + P.list);
-  uint32_t* bm = sw + P.bm;
-  float* scr = smem_raw + P.scr + warp * 32;
-  float* score = smem_raw + P.score;
-  float* mval = smem_raw + P.mval;
-  int* midx = reinterpret_cast<int*>(smem_raw + P.midx);
-  int* misc = reinterpret_cast<int*>(smem_raw + P.misc);
-  const int cp = a.cp;
   const int h = H > 0 ? H : a.h;
-  const int nwords = cp / 32;
-  const int n_union = (a.rows > nw ? a.rows : nw) * cp;
+  const WarpPlan P = warp_plan(S, h, a.ncell);
+  double2* lnt = reinterpret_cast<double2*>(smem_raw);
+  float* kw_s = smem_raw + kLnTableSize * 4;
+  float* wb = smem_raw + kBlockHeaderWords + warp * P.total;
+  float* row = wb + P.row;
+  uint32_t* tags = reinterpret_cast<uint32_t*>(wb + P.tags);
+  uint32_t* bm = reinterpret_cast<uint32_t*>(wb + P.bm);
+  float* scr = wb + P.scr;
+  float* score = wb + P.score;
+  float* mval = wb + P.mval;
+  int* midx = reinterpret_cast<int*>(wb + P.midx);
 
   for (int i = threadIdx.x; i < kLnTableSize; i += blockDim.x) lnt[i] = a.ln_tab[i];
   for (int i = threadIdx.x; i <= a.h; i += blockDim.x) kw_s[i] = a.kw[i];
+  for (int i = lane; i < a.ncell; i += 32) tags[i] = 0u;
+  __syncthreads();
   Counters k;
+  uint32_t seq = 1;
 
   for (;;) {
-    if (threadIdx.x == 0) misc[0] = (int)atomicAdd(a.work, 1u);
-    __syncthreads();
-    const int64_t p = misc[0];
-    __syncthreads();
-    if (p >= a.n_prec) break;
+    unsigned long long pw = 0;
+    if (lane == 0) pw = atomicAdd(a.work, 1ull);
+    pw = __shfl_sync(kFull, pw, 0);
+    if (pw >= (unsigned long long)a.n_prec) break;
+    const int64_t p = (int64_t)pw;
     const int F = a.nf[p];
     const int cs = a.cs[p], ce = a.ce[p];
     const int C = ce - cs;
     if (F == 0 || C <= 0) {
-      if (threadIdx.x == 0) a.cand_n[p] = 0;
+      if (lane == 0) a.cand_n[p] = 0;
       continue;
     }
     if (C > a.c_max) {
-      if (threadIdx.x == 0) {
+      if (lane == 0) {
         a.cand_n[p] = 0;
         atomicOr(a.err, 2);
       }
       continue;
     }
     const int nwin = a.nwin[p];
-    if (warp == 0 && lane == 0) k.frag += F;
+    const int npairs = F * nwin;
+    const int passes = (C + 32 * S - 1) / (32 * S);
+    k.frag += F;
+    for (int i = lane; i <= C + C / S; i += 32) score[i] = 0.0f;  // cycles [0, C) with pads
+    if (seq >= (1u << 26)) {  // keep tag << 5 inside 32 bits
+      __syncwarp();
+      for (int i = lane; i < a.ncell; i += 32) tags[i] = 0u;
+      seq = 1;
+    }
 
-    for (int r0 = 0; r0 < F; r0 += a.rows) {
-      const int nr = min(a.rows, F - r0);
-      // zero the XIC rows, the convolved rows (which also clears the gather tags)
-      // and the bitmaps
+    // CSR offsets of up to 32 (fragment, window) pairs, fetched together
+    int pb = -64;
+    int64_t rs = 0, re = 0;
+    uint32_t b0 = 0, b1 = 0;
+    int wsel = 0;
+    for (int f = 0; f < F; ++f) {
       {
-        float4* x4 = reinterpret_cast<float4*>(xrow);
-        const int nx4 = nr * row_stride(cp) / 4;
-        for (int i = threadIdx.x; i < nx4; i += blockDim.x) x4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        float4* v4 = reinterpret_cast<float4*>(vrow);
-        for (int i = threadIdx.x; i < n_union / 4; i += blockDim.x) v4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int i = threadIdx.x; i < nr * P.bw; i += blockDim.x) bm[i] = 0u;
-        if (threadIdx.x == 0) misc[2] = 0;
+        float4* r4 = reinterpret_cast<float4*>(row);
+        for (int i = lane; i < P.row_words / 4; i += 32) r4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int i = lane; i < P.bw; i += 32) bm[i] = 0u;
       }
-      __syncthreads();
-      // ---- 1. gather: this warp's rows, all their windows
-      {
-        uint32_t seq = 1;
-        const int my_rows = nr > warp ? (nr - warp + nw - 1) / nw : 0;
-        const int n_pairs = my_rows * nwin;
-        for (int pb = 0; pb < n_pairs; pb += 32) {
-          // CSR offsets of up to 32 pairs in one round trip
-          int64_t rs = 0, re = 0;
-          uint32_t b0 = 0, b1 = 0;
-          const int pi = pb + lane;
-          if (pi < n_pairs) {
-            const int f = r0 + warp + (pi / nwin) * nw;
-            const int wi = pi % nwin;
-            const int64_t fo = p * a.kf + f;
+      __syncwarp();
+      // ---- 1. gather: the fragment's pairs in window order
+      const unsigned long long acc0 = k.acc;
+      for (int wi = 0; wi < nwin; ++wi) {
+        const int pi = f * nwin + wi;
+        if (pi >= pb + 32) {
+          pb = pi;
+          const int pj = pb + lane;
+          rs = re = 0;
+          b0 = b1 = 0;
+          wsel = 0;
+          if (pj < npairs) {
+            const int fj = pj / nwin, wj = pj - fj * nwin;
+            const int64_t fo = p * a.kf + fj;
             b0 = a.blo[fo];
             b1 = a.bhi[fo];
+            wsel = a.wins[p * a.maxw + wj];
             if (b1 > b0) {
-              const WinInfo w = a.win[a.wins[p * a.maxw + wi]];
+              const WinInfo w = a.win[wsel];
               rs = __ldg(a.ss + w.ss_off + b0);
               re = __ldg(a.ss + w.ss_off + b1);
             }
           }
-          const int np = min(32, n_pairs - pb);
-          for (int q = 0; q < np; ++q) {
-            const int64_t qrs = __shfl_sync(kFull, rs, q);
-            const int64_t qre = __shfl_sync(kFull, re, q);
-            const uint32_t qb0 = __shfl_sync(kFull, b0, q);
-            const uint32_t qb1 = __shfl_sync(kFull, b1, q);
-            if (qb1 <= qb0) continue;
-            const int pq = pb + q;
-            const int fl = warp + (pq / nwin) * nw;  // row within the round
-            const WinInfo w = a.win[a.wins[p * a.maxw + pq % nwin]];
-            k.off += 2;
-            k.pairs += 1;
-            k.bins1 += qb1 - qb0 + 1;
-            gather_pair(a, w, qb0, qb1, qrs, qre, cs, ce, lane, xrow + (size_t)fl * row_stride(cp),
-                        bm + fl * P.bw, tags, scr, seq, k);
-          }
         }
+        const int q = pi - pb;
+        const int64_t qrs = __shfl_sync(kFull, rs, q);
+        const int64_t qre = __shfl_sync(kFull, re, q);
+        const uint32_t qb0 = __shfl_sync(kFull, b0, q);
+        const uint32_t qb1 = __shfl_sync(kFull, b1, q);
+        const int qw = __shfl_sync(kFull, wsel, q);
+        if (qb1 <= qb0) continue;
+        const WinInfo w = a.win[qw];
+        k.off += 2;
+        k.pairs += 1;
+        k.bins1 += qb1 - qb0 + 1;
+        gather_pair<S>(a, w, qb0, qb1, qrs, qre, cs, ce, lane, row, P.off, bm, tags, scr, seq, k);
       }
-      __syncthreads();
-      // ---- 2. list of the outputs with a nonzero input window
-      for (int it = threadIdx.x; it < nr * nwords; it += blockDim.x) {
-        const int fl = it / nwords, w = it - fl * nwords;
-        uint32_t act = active_word(bm + fl * P.bw, w, h, C);
-        if (act) {
-          int pos = atomicAdd(&misc[2], __popc(act));
-          while (act) {
-            const int b = __ffs(act) - 1;
-            list[pos++] = (uint16_t)((fl << kListRowShift) | (w * 32 + b));
-            act &= act - 1;
-          }
-        }
-      }
-      // the tags region becomes the convolved rows: clear what the gather left
-      for (int i = threadIdx.x; i < nw * cp; i += blockDim.x) vrow[i] = 0.0f;
-      __syncthreads();
-      // ---- 3. convolution of the listed outputs
-      const int n_list = misc[2];
-      for (int it = threadIdx.x; it < n_list; it += blockDim.x) {
-        const int e = list[it];
-        const int fl = e >> kListRowShift, j = e & ((1 << kListRowShift) - 1);
-        vrow[(size_t)fl * cp + j] =
-            conv_output<H>(a, xrow + (size_t)fl * row_stride(cp), bm + fl * P.bw, kw_s, j);
-      }
-      __syncthreads();
-      // ---- 4. score[j] += ln(conv_f[j] + 1) * w_f in fragment order
-      // (src/score/scalar.rs:16-22); a zero conv adds ln(1) * w = +0 and is skipped
-      const float* fw = a.fw + p * a.kf + r0;
-      for (int j = threadIdx.x; j < C; j += blockDim.x) {
-        float acc = r0 == 0 ? 0.0f : score[j];
-        for (int q = 0; q < nr; ++q) {
-          const float c = vrow[(size_t)q * cp + j];
-          if (c != 0.0f) acc = __fadd_rn(acc, __fmul_rn(ln_fast(__fadd_rn(c, 1.0f), lnt), __ldg(fw + q)));
-        }
-        score[j] = acc;
-      }
-      __syncthreads();
-    }
-
-    // strict 5-point local maxima (src/peak_group_selection/mod.rs:33-43)
-    if (threadIdx.x == 0) misc[1] = 0;
-    __syncthreads();
-    for (int i = threadIdx.x + 2; i < C - 2; i += blockDim.x) {
-      if (score[i - 2] < score[i - 1] && score[i - 1] < score[i] && score[i] > score[i + 1] &&
-          score[i + 1] > score[i + 2]) {
-        const int slot = atomicAdd(&misc[1], 1);
-        if (slot < P.mx) {
-          mval[slot] = score[i];
-          midx[slot] = i;
-        }
-      }
-    }
-    __syncthreads();
-    // top-K by (value descending, cycle ascending): the reference's stable sort by
-    // value of maxima found in cycle order (src/peak_group_selection/mod.rs:45-61).
-    if (warp == 0) {
-      const int nmax = min(misc[1], P.mx);
-      if (misc[1] > P.mx && lane == 0) atomicOr(a.err, 4);
-      const int kk = min(a.k_out, nmax);
-      for (int r = 0; r < kk; ++r) {
-        float bv = 0.0f;
-        int bi = -1, bk = -1;
-        for (int q = lane; q < nmax; q += 32) {
-          const float v = mval[q];
-          const int i = midx[q];
-          if (v != v) continue;  // already taken
-          if (bk < 0 || v > bv || (v == bv && i < bi)) {
-            bv = v;
-            bi = i;
-            bk = q;
-          }
-        }
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-          const float ov = __shfl_xor_sync(kFull, bv, o);
-          const int oi = __shfl_xor_sync(kFull, bi, o);
-          const int ok = __shfl_xor_sync(kFull, bk, o);
-          if (ok >= 0 && (bk < 0 || ov > bv || (ov == bv && oi < bi))) {
-            bv = ov;
-            bi = oi;
-            bk = ok;
-          }
-        }
-        if (lane == 0) {
-          a.cand_score[p * a.k_out + r] = bv;
-          a.cand_center[p * a.k_out + r] = cs + bi;
-          mval[bk] = __int_as_float(0x7fc00000);
+      __syncwarp();
+      const float wf = __ldg(a.fw + p * a.kf + f);
+      if (!isfinite(wf)) {
+        // ln(conv + 1) * inf is NaN even where conv is zero: every column takes
+        // its term, as in the reference
+        for (int j = lane; j < C; j += 32) {
+          const float c = (j >= h && j < C - h) ? conv_at<S>(row, P.off, kw_s, h, j) : 0.0f;
+          score_add(score, xaddr<S>(j), c, wf, lnt);
         }
         __syncwarp();
+        continue;
       }
-      if (lane == 0) a.cand_n[p] = kk;
+      if (k.acc == acc0) continue;  // empty row: every term is +0
+      // ---- 2./3. convolution of this lane's cycles and their score terms; a zero
+      // output adds ln(1) * w = +0 and is skipped
+      for (int ps = 0; ps < passes; ++ps) {
+        const int j0 = ps * 32 * S + lane * S;
+        if (j0 + S <= h || j0 >= C - h) continue;  // no valid output [h, C - h) here
+        if (!bits_any(bm, j0 - h + kBitOff, S + 2 * h)) continue;
+        if (H > 0) {
+          // cycle j0 + u sits at rb[u + floor(u / S)]; its score at sb[u] (0 <= u < S)
+          const float* rb = row + (ps * 32 + lane + P.off / S) * (S + 1);
+          float* sb = score + (ps * 32 + lane) * (S + 1);
+          float x[S + 2 * H];
+#pragma unroll
+          for (int t = 0; t < S + 2 * H; ++t) x[t] = rb[(t - H) + floordiv(t - H, S)];
+#pragma unroll
+          for (int m = 0; m < S; ++m) {
+            const int j = j0 + m;
+            float s = __fadd_rn(0.0f, __fmul_rn(x[m + H], a.kw[H]));
+#pragma unroll
+            for (int t = 0; t < H; ++t)
+              s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[m + t], x[m + 2 * H - t]), a.kw[t]));
+            if (s != 0.0f && j >= H && j < C - H) score_add(sb, m, s, wf, lnt);
+          }
+        } else {
+          for (int m = 0; m < S; ++m) {
+            const int j = j0 + m;
+            if (j < h || j >= C - h) continue;
+            const float s = conv_at<S>(row, P.off, kw_s, h, j);
+            if (s != 0.0f) score_add(score, xaddr<S>(j), s, wf, lnt);
+          }
+        }
+      }
+      __syncwarp();
     }
-    __syncthreads();
+    __syncwarp();
+
+    // ---- strict 5-point local maxima (src/peak_group_selection/mod.rs:33-43), kept
+    // in cycle order: per pass, lane l's maxima go after those of lanes < l
+    int nmax = 0;
+    for (int ps = 0; ps < passes; ++ps) {
+      const int seg = ps * 32 + lane;
+      const float* sb = score + seg * (S + 1);
+      uint32_t mk = 0;
+      if (seg * S < C - 2 && seg * S + S > 2) {
+        float v[S + 4];
+#pragma unroll
+        for (int t = 0; t < S + 4; ++t) v[t] = sb[(t - 2) + floordiv(t - 2, S)];
+#pragma unroll
+        for (int m = 0; m < S; ++m) {
+          const int i = seg * S + m;
+          const bool is = i >= 2 && i < C - 2 && v[m] < v[m + 1] && v[m + 1] < v[m + 2] &&
+                          v[m + 2] > v[m + 3] && v[m + 3] > v[m + 4];
+          mk |= (uint32_t)is << m;
+        }
+      }
+      const int cnt = __popc(mk);
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+      }
+      int pos = nmax + incl - cnt;
+      while (mk) {
+        const int m = __ffs(mk) - 1;
+        if (pos < P.mx) {
+          mval[pos] = sb[m];
+          midx[pos] = seg * S + m;
+        }
+        ++pos;
+        mk &= mk - 1;
+      }
+      nmax += __shfl_sync(kFull, incl, 31);
+    }
+    __syncwarp();
+    if (nmax > P.mx) {  // cannot happen: maxima are at least 4 cycles apart
+      if (lane == 0) atomicOr(a.err, 4);
+      nmax = P.mx;
+    }
+    // top-K by (value descending, cycle ascending): the reference's stable sort by
+    // value of maxima found in cycle order (src/peak_group_selection/mod.rs:45-61).
+    const int kk = min(a.k_out, nmax);
+    for (int r = 0; r < kk; ++r) {
+      float bv = 0.0f;
+      int bi = -1, bk = -1;
+      for (int q = lane; q < nmax; q += 32) {
+        const float v = mval[q];
+        const int i = midx[q];
+        if (v != v) continue;  // already taken
+        if (bk < 0 || v > bv || (v == bv && i < bi)) {
+          bv = v;
+          bi = i;
+          bk = q;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o >= 1; o >>= 1) {
+        const float ov = __shfl_xor_sync(kFull, bv, o);
+        const int oi = __shfl_xor_sync(kFull, bi, o);
+        const int ok = __shfl_xor_sync(kFull, bk, o);
+        if (ok >= 0 && (bk < 0 || ov > bv || (ov == bv && oi < bi))) {
+          bv = ov;
+          bi = oi;
+          bk = ok;
+        }
+      }
+      if (lane == 0) {
+        a.cand_score[p * a.k_out + r] = bv;
+        a.cand_center[p * a.k_out + r] = cs + bi;
+        mval[bk] = __int_as_float(0x7fc00000);
+      }
+      __syncwarp();
+    }
+    if (lane == 0) a.cand_n[p] = kk;
   }
   if (a.stats && lane == 0) {
     atomicAdd(a.stats + 0, k.pairs);

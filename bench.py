@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warps-per-block", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--cycles-per-lane", type=int, default=0)
     return ap.parse_args()
 
 
@@ -382,6 +383,7 @@ def run_ours(args, rank, world, local_rank):
 
     sel = ads.PeakGroupSelection(params, verbose=False, device=local_rank, time_stages=True,
                                  warps_per_block=args.warps_per_block,
+                                 cycles_per_lane=args.cycles_per_lane,
                                  blocks_per_sm=args.blocks_per_sm)
     cand = sel.new_candidates()
     stream = torch.cuda.ExternalStream(sel.stream, device=device)

@@ -167,6 +167,8 @@ typedef struct {
   int32_t gather_mode;     /* 0 = automatic, 1 = always scan bin ranges, 2 = always
                               binary-search each bin (both are exact; for testing) */
   int32_t time_stages;     /* 1: record CUDA events around each stage of a search */
+  int32_t cycles_per_lane; /* 0 = chosen from the longest RT window; else 4, 8, 10, 13
+                              or 16 consecutive cycles per lane of the search kernel */
   int64_t stream;          /* cudaStream_t to run on, 0 = the handle's own stream */
 } AdsEngineOptions;
 

@@ -53,6 +53,16 @@ def test_search_bit_exact_vs_rn_oracle(workload, gather_mode):
     assert_candidates_equal(got, ref, exact_scores=True, where=f"{cfg.name}/mode{gather_mode}")
 
 
+@pytest.mark.parametrize("cycles_per_lane", [4, 8, 10, 13, 16])
+def test_search_bit_exact_every_lane_width(workload, cycles_per_lane):
+    """Every compiled cycles-per-lane instance gives the same bits (one pass or
+    several per RT window)."""
+    cfg, run, la, (od, ol, tol) = workload
+    got, *_ = product_search(run, la, cfg.params_dict(), cycles_per_lane=cycles_per_lane)
+    ref = oracle_search(run, la, cfg.params_dict(), oracle.LOG_RN, od, ol, tol)
+    assert_candidates_equal(got, ref, exact_scores=True, where=f"{cfg.name}/S{cycles_per_lane}")
+
+
 def test_search_vs_reference_numerics(workload):
     cfg, run, la, (od, ol, tol) = workload
     got, *_ = product_search(run, la, cfg.params_dict())
@@ -73,6 +83,9 @@ def test_search_deterministic(workload):
     dict(peak_length=15),              # center - peak_length wraps as usize
     dict(kernel_size=9, fwhm_rt=2.0),
     dict(kernel_size=62),              # largest supported kernel
+    dict(kernel_size=21),              # unrolled stencil, half width 11
+    dict(kernel_size=31, fwhm_rt=7.0), # unrolled stencil, half width 16
+    dict(kernel_size=14),              # generic stencil, half width 7
     dict(candidate_count=0),
     dict(candidate_count=50),
     dict(top_k_fragments=0),
@@ -91,6 +104,22 @@ def test_edge_cases(variant):
     assert_candidates_equal(got, ref, exact_scores=True, where=str(variant))
     ref_g = oracle_search(run, la, params, oracle.LOG_GLIBC)
     assert_candidates_equal(got, ref_g, exact_scores=False, where=str(variant))
+
+
+@pytest.mark.parametrize("value", [np.inf, 1e-30])
+def test_extreme_library_intensity(value):
+    """An infinite library intensity makes ln(0 + 1) * inf = NaN in every column
+    of the score, as in the reference; a tiny one only scales its row."""
+    run, la = edge_case_workload()
+    la = dict(la)
+    fi = np.array(la["fragment_intensity"], dtype=np.float32, copy=True)
+    fi[1] = value
+    la["fragment_intensity"] = fi
+    params = dict(fwhm_rt=3.0, kernel_size=20, peak_length=5, mass_tolerance=20.0,
+                  rt_tolerance=30.0, candidate_count=3, top_k_fragments=6)
+    got, *_ = product_search(run, la, params)
+    ref = oracle_search(run, la, params, oracle.LOG_RN)
+    assert_candidates_equal(got, ref, exact_scores=True, where=f"intensity {value}")
 
 
 def test_edge_case_csr():
