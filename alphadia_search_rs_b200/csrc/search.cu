@@ -16,6 +16,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 
 #include "common.cuh"
@@ -991,3 +992,265 @@ int ads_candidates_destroy(AdsCandidates* c) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------- allocation-free search
+//
+// ads_select_noalloc serves callers that may not allocate device memory at search
+// time: processes whose device memory belongs to another allocator (a framework's
+// caching allocator, a serving process on a fixed memory budget), where a
+// cudaMalloc from this library could fail or fragment that memory, and loops that
+// cannot afford cudaFree's implicit device-wide synchronisation.  Its working
+// memory is the fixed array below, which exists once in every GPU context that
+// loads this library, for the life of the process.
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[ADS_NOALLOC_SCRATCH_BYTES];
+
+namespace ads {
+namespace {
+
+constexpr size_t kNoAllocLnBytes = kLnTableSize * sizeof(double2);  // first 4 KiB: ln table
+
+std::mutex g_noalloc_mu;
+std::map<int, char*> g_noalloc_base;  // device -> device address of g_noalloc_scratch
+
+// The scratch array's device address on the current device, set up on first use:
+// host code only knows the array through a stand-in symbol, so the address comes
+// from cudaGetSymbolAddress (with the device current), and the ln table is copied
+// into the array's first 4 KiB.  The device must be current.
+int noalloc_scratch(int device, char** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  auto it = g_noalloc_base.find(device);
+  if (it != g_noalloc_base.end()) {
+    *out = it->second;
+    return ADS_OK;
+  }
+  void* p = nullptr;
+  ADS_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+  const std::vector<double2> tab = host_ln_table();
+  ADS_CUDA(cudaMemcpy(p, tab.data(), kNoAllocLnBytes, cudaMemcpyHostToDevice));
+  g_noalloc_base[device] = static_cast<char*>(p);
+  *out = static_cast<char*>(p);
+  return ADS_OK;
+}
+
+// Bump allocator over the scratch array (256-byte aligned pieces); `end` tells
+// whether everything fitted.
+struct ScratchCarver {
+  char* base;
+  size_t off;
+  template <class T>
+  T* take(int64_t n) {
+    T* p = reinterpret_cast<T*>(base + off);
+    off += ((size_t)std::max<int64_t>(n, 1) * sizeof(T) + 255) / 256 * 256;
+    return p;
+  }
+};
+
+int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* params,
+                   int64_t stream, int64_t capacity, uint64_t* o_pidx, uint64_t* o_rank,
+                   float* o_score, uint64_t* o_center, uint64_t* o_start, uint64_t* o_stop,
+                   int64_t* o_count, int32_t* o_flags) {
+  if (!d || !l || !params || !o_count) return fail(ADS_ERR_INVALID_ARGUMENT, "null argument");
+  if (d->device != l->device) return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
+  std::vector<float> kernel;
+  int h = 0;
+  ADS_TRY(check_params(*params, &kernel, &h));
+  const AdsSelectionParams& prm = *params;
+  DeviceGuard dg(d->device);
+  char* base = nullptr;
+  ADS_TRY(noalloc_scratch(d->device, &base));
+  const cudaStream_t st = (cudaStream_t)stream;
+
+  // the same launch shape as ads_select with default engine options
+  const int64_t P = l->n_prec;
+  const int L = (int)kernel.size();
+  const int64_t n_rt = (int64_t)d->rt.size();
+  const float tol_max = l->has_tol ? std::max(l->max_tol, 0.0f) : prm.rt_tolerance;
+  const int64_t c_max = std::max<int64_t>(1, max_cycle_span(d->rt, d->delta_t, tol_max, prm.kernel_size));
+  if (c_max > kMaxCycles)
+    return fail(ADS_ERR_INVALID_ARGUMENT, "RT windows longer than 2048 cycles are not supported (" +
+                                              std::to_string(c_max) + " cycles)");
+  int S = kLaneCycles[0];
+  int64_t best = -1;
+  for (int cand : kLaneCycles) {
+    const int64_t slots = (c_max + 32 * cand - 1) / (32 * cand) * 32 * cand;
+    if (best < 0 || slots <= best) {
+      best = slots;
+      S = cand;
+    }
+  }
+  const int ncell = (int)((c_max + 32 * S - 1) / (32 * S) * 32 * S);
+  const int k_out = (int)std::max<int64_t>(0, std::min<int64_t>(prm.candidate_count, maxima_cap(ncell)));
+  const int kf = (int)std::max<int64_t>(1, std::min<int64_t>(prm.top_k_fragments, l->max_frag));
+  const int maxw = std::max(1, d->max_overlap);
+  const int64_t rows_needed = P * (int64_t)k_out;
+  if (capacity < rows_needed)
+    return fail(ADS_ERR_INVALID_ARGUMENT,
+                "output capacity " + std::to_string(capacity) + " is below precursors x candidates = " +
+                    std::to_string(rows_needed));
+  if (rows_needed > 0 && (!o_pidx || !o_rank || !o_score || !o_center || !o_start || !o_stop))
+    return fail(ADS_ERR_INVALID_ARGUMENT, "null output array");
+
+  // scratch layout after the ln table
+  int n_sms = 0;
+  ADS_CUDA(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, d->device));
+  const int64_t prep_blocks = std::min<int64_t>((P * 32 + kPrepThreads - 1) / kPrepThreads,
+                                                 (int64_t)n_sms * 16);
+  const int64_t keep_stride = std::max<int64_t>(l->max_frag, 1);
+  const int64_t nb = (P + kScanBlock - 1) / kScanBlock;
+  ScratchCarver sc{base, kNoAllocLnBytes};
+  auto* work = sc.take<unsigned long long>(1);
+  auto* err = sc.take<int>(1);
+  auto* nf = sc.take<int>(P);
+  auto* cs = sc.take<int>(P);
+  auto* ce = sc.take<int>(P);
+  auto* nwin = sc.take<int>(P);
+  auto* wins = sc.take<int>(P * maxw);
+  auto* fw = sc.take<float>(P * kf);
+  auto* blo = sc.take<uint32_t>(P * kf);
+  auto* bhi = sc.take<uint32_t>(P * kf);
+  auto* keep = sc.take<uint8_t>(prep_blocks * (kPrepThreads / 32) * keep_stride);
+  auto* cand_n = sc.take<int>(P);
+  auto* cand_score = sc.take<float>(P * k_out);
+  auto* cand_center = sc.take<int>(P * k_out);
+  auto* block_sums = sc.take<int64_t>(nb);
+  if (sc.off > (size_t)ADS_NOALLOC_SCRATCH_BYTES)
+    return fail(ADS_ERR_INVALID_ARGUMENT,
+                "this search needs " + std::to_string(sc.off) + " bytes of scratch, more than the " +
+                    std::to_string((size_t)ADS_NOALLOC_SCRATCH_BYTES) +
+                    " of ads_select_noalloc; search the library in smaller parts");
+  int* flags = o_flags ? reinterpret_cast<int*>(o_flags) : err;
+
+  // what must start at zero: the work counter, the error flags and the count
+  ADS_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
+  ADS_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), st));
+  ADS_CUDA(cudaMemsetAsync(o_count, 0, sizeof(int64_t), st));
+  if (P == 0 || k_out == 0) return ADS_OK;
+
+  // the grid exists: building `d` uploaded it to this device
+  GridView g;
+  ADS_TRY(device_grid(d->device, &g));
+  PrepArgs pa;
+  pa.n_prec = P;
+  pa.pmz = l->pmz_p;
+  pa.prt = l->prt_p;
+  pa.ptol = l->has_tol ? l->ptol_p : nullptr;
+  pa.rt_tol = prm.rt_tolerance;
+  pa.fstart = l->fstart_p;
+  pa.fstop = l->fstop_p;
+  pa.fmz = l->fmz_p;
+  pa.fint = l->fint_p;
+  pa.fnum = l->fnum_p;
+  pa.ftype = l->ftype_p;
+  pa.rt = d->rt_dev.p;
+  pa.n_rt = (int)n_rt;
+  pa.delta_t = d->delta_t;
+  pa.pad = (float)prm.kernel_size;
+  pa.win = d->win_dev.p;
+  pa.n_obs = (int)d->n_obs;
+  pa.g = g;
+  pa.mass_tol = prm.mass_tolerance;
+  pa.top_k = (int)std::min<int64_t>(prm.top_k_fragments, (int64_t)1 << 30);
+  pa.kf = kf;
+  pa.maxw = maxw;
+  pa.min_c = std::max(L + 1, 5);
+  pa.keep = keep;
+  pa.keep_stride = keep_stride;
+  pa.nf = nf;
+  pa.cs = cs;
+  pa.ce = ce;
+  pa.nwin = nwin;
+  pa.wins = wins;
+  pa.fw = fw;
+  pa.blo = blo;
+  pa.bhi = bhi;
+  pa.err = flags;
+  prep_kernel<<<(int)prep_blocks, kPrepThreads, 0, st>>>(pa);
+  ADS_LAUNCH_CHECK();
+
+  int nw = 8;
+  int max_smem = 0;
+  ADS_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
+  while (nw > 1 && search_smem_bytes(nw, S, h, ncell) > (size_t)max_smem) --nw;
+  const size_t smem = search_smem_bytes(nw, S, h, ncell);
+  if (smem > (size_t)max_smem)
+    return fail(ADS_ERR_INVALID_ARGUMENT, "RT window too long for shared memory (" +
+                                              std::to_string(c_max) + " cycles)");
+  void (*kern)(SearchArgs) = pick_search_kernel(h, S);
+  ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
+  if (occ <= 0) return fail(ADS_ERR_INTERNAL, "search kernel cannot be resident");
+  SearchArgs sa;
+  std::memset(&sa, 0, sizeof(sa));
+  sa.n_prec = P;
+  sa.nf = nf;
+  sa.cs = cs;
+  sa.ce = ce;
+  sa.nwin = nwin;
+  sa.wins = wins;
+  sa.maxw = maxw;
+  sa.fw = fw;
+  sa.blo = blo;
+  sa.bhi = bhi;
+  sa.kf = kf;
+  sa.win = d->win_dev.p;
+  sa.ss = d->slice_starts.p;
+  sa.cyc = d->cycles.p;
+  sa.inten = d->intens.p;
+  sa.ln_tab = reinterpret_cast<const double2*>(base);
+  for (int k = 0; k <= h; ++k) sa.kw[k] = kernel[k];
+  sa.h = h;
+  sa.k_out = k_out;
+  sa.c_max = (int)c_max;
+  sa.ncell = ncell;
+  sa.gather_mode = 0;
+  sa.scan_thresh = 4 * 32 * kPrefetchChunks;
+  sa.work = work;
+  sa.err = flags;
+  sa.cand_n = cand_n;
+  sa.cand_score = cand_score;
+  sa.cand_center = cand_center;
+  sa.stats = nullptr;
+  const int64_t blocks = std::min<int64_t>((int64_t)n_sms * occ, (P + nw - 1) / nw);
+  kern<<<(int)blocks, nw * 32, smem, st>>>(sa);
+  ADS_LAUNCH_CHECK();
+
+  block_sum_kernel<<<(int)nb, kScanBlock, 0, st>>>(cand_n, P, block_sums);
+  ADS_LAUNCH_CHECK();
+  scan_block_sums_kernel<<<1, kScanBlock, 0, st>>>(block_sums, nb, o_count);
+  ADS_LAUNCH_CHECK();
+  ScatterArgs ca;
+  ca.n_prec = P;
+  ca.k_out = k_out;
+  ca.peak_length = (uint64_t)prm.peak_length;
+  ca.rt_len = (uint64_t)n_rt;
+  ca.cand_n = cand_n;
+  ca.cand_score = cand_score;
+  ca.cand_center = cand_center;
+  ca.pidx = l->pidx_p;
+  ca.block_off = block_sums;
+  ca.o_pidx = o_pidx;
+  ca.o_rank = o_rank;
+  ca.o_score = o_score;
+  ca.o_center = o_center;
+  ca.o_start = o_start;
+  ca.o_stop = o_stop;
+  scatter_kernel<<<(int)nb, kScanBlock, 0, st>>>(ca);
+  ADS_LAUNCH_CHECK();
+  return ADS_OK;
+}
+
+}  // namespace
+}  // namespace ads
+
+extern "C" int ads_select_noalloc(const AdsDia* dia, const AdsLib* lib,
+                                  const AdsSelectionParams* params, int64_t stream,
+                                  int64_t capacity, uint64_t* precursor_idx, uint64_t* rank,
+                                  float* score, uint64_t* cycle_center, uint64_t* cycle_start,
+                                  uint64_t* cycle_stop, int64_t* count, int32_t* flags) {
+  return ads::guarded([&] {
+    return ads::select_noalloc(dia, lib, params, stream, capacity, precursor_idx, rank, score,
+                               cycle_center, cycle_start, cycle_stop, count, flags);
+  });
+}

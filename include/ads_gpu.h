@@ -202,6 +202,36 @@ int ads_select(AdsSelection* sel, const AdsDia* dia, const AdsLib* lib, AdsCandi
  * size is read (and the stream synchronised) by ads_candidates_size. */
 int ads_select_async(AdsSelection* sel, const AdsDia* dia, const AdsLib* lib,
                      AdsCandidates* reuse);
+/* Allocation-free search.  No counterpart in the reference: an addition for callers
+ * that may not allocate device memory while they search -- processes whose device
+ * memory belongs to another allocator (a framework's caching allocator, a serving
+ * process on a fixed budget), where an allocation from this library could fail or
+ * fragment that memory, and loops that cannot afford cudaFree's implicit
+ * device-wide synchronisation.
+ *
+ * Runs the search of ads_select with default engine options and writes the
+ * candidates, in the same order and with the same values, into caller-owned
+ * device arrays of `capacity` rows (capacity >= precursors x min(candidate_count,
+ * maxima capacity)); the row count goes to the device int64 *count, the kernels'
+ * internal error flags (0 = none) to the device int32 *flags when it is not NULL.
+ * The scan_* columns of the reference are zero and not written.  Everything is
+ * enqueued on `stream` (a cudaStream_t as integer, 0 = the legacy default stream)
+ * and the call returns without waiting.
+ *
+ * Working memory is a fixed device array of ADS_NOALLOC_SCRATCH_BYTES that every
+ * GPU context loading this library holds until the process exits; a search that
+ * needs more (about 200 bytes per precursor with 12 fragments and 3 candidates)
+ * fails with ADS_ERR_INVALID_ARGUMENT and should be split over smaller libraries.
+ * The first call on a device sets the array up (looks up its device address and
+ * copies a 4 KiB table into it, synchronously); make that first call before any
+ * stream capture.  Calls whose work overlaps on the GPU share the array and race:
+ * issue them on one stream or order them with events. */
+#define ADS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int ads_select_noalloc(const AdsDia* dia, const AdsLib* lib, const AdsSelectionParams* params,
+                       int64_t stream, int64_t capacity, uint64_t* precursor_idx, uint64_t* rank,
+                       float* score, uint64_t* cycle_center, uint64_t* cycle_start,
+                       uint64_t* cycle_stop, int64_t* count, int32_t* flags);
+
 /* Empty collection bound to a selection's device, for ads_select_async. */
 int ads_candidates_create(const AdsSelection* sel, AdsCandidates** out);
 /* cudaStream_t (as integer) that a selection enqueues its work on. */
