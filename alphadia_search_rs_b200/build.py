@@ -28,6 +28,9 @@ LIBNAME = "libads_gpu.so"
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
+    # no implicit multiply-add contraction anywhere in device code (the parity
+    # arithmetic uses explicitly rounded ops; this keeps everything else alike)
+    "-fmad=false",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
     "-Xptxas", "-warn-spills",
     "-diag-suppress", "1444",  # deprecated cub iterators

@@ -14,10 +14,13 @@
 //                       candidates into the nine to_arrays() columns.
 #include <algorithm>
 #include <array>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
+
+#include <cuda_bf16.h>
 
 #include "common.cuh"
 
@@ -295,25 +298,70 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a) {
 // unrolled stencils for the half widths of kernel_size 20, 21-22 and 31-32, any
 // other half width through the generic path.
 constexpr int kLaneCycles[] = {4, 8, 10, 13, 16};
+constexpr int kMaxClasses = 6;
 
-template <int H>
+// Length classes of one search: class b covers C <= bound[b] with S[b] cycles per
+// lane (bound[last] = the longest window, searched in one or more passes).
+struct LenClasses {
+  int bound[kMaxClasses];
+  int S[kMaxClasses];
+};
+
+// The fewest lane slots (passes * 32 * S) covering c cycles, ties to the larger S.
+int best_lane_cycles(int64_t c) {
+  int S = kLaneCycles[0];
+  int64_t best = -1;
+  for (int cand : kLaneCycles) {
+    const int64_t slots = (c + 32 * cand - 1) / (32 * cand) * 32 * cand;
+    if (best < 0 || slots <= best) {
+      best = slots;
+      S = cand;
+    }
+  }
+  return S;
+}
+
+// One class per lane width whose single pass is shorter than the longest window,
+// then one for the rest.  A fixed cycles_per_lane gives a single class.
+int plan_classes(int64_t c_max, int fixed_S, LenClasses* out) {
+  int n = 0;
+  if (fixed_S == 0) {
+    for (int s : kLaneCycles)
+      if (32 * (int64_t)s < c_max) {
+        out->bound[n] = 32 * s;
+        out->S[n] = s;
+        ++n;
+      }
+  }
+  out->bound[n] = (int)c_max;
+  out->S[n] = fixed_S ? fixed_S : best_lane_cycles(c_max);
+  return n + 1;
+}
+
+template <int H, bool FAST>
 void (*pick_for_h(int S))(SearchArgs) {
   switch (S) {
-    case 4: return search_kernel<H, 4>;
-    case 8: return search_kernel<H, 8>;
-    case 10: return search_kernel<H, 10>;
-    case 13: return search_kernel<H, 13>;
-    default: return search_kernel<H, 16>;
+    case 4: return search_kernel<H, 4, FAST>;
+    case 8: return search_kernel<H, 8, FAST>;
+    case 10: return search_kernel<H, 10, FAST>;
+    case 13: return search_kernel<H, 13, FAST>;
+    default: return search_kernel<H, 16, FAST>;
   }
 }
 
-void (*pick_search_kernel(int h, int S))(SearchArgs) {
+template <bool FAST>
+void (*pick_for_precision(int h, int S))(SearchArgs) {
   switch (h) {
-    case 10: return pick_for_h<10>(S);
-    case 11: return pick_for_h<11>(S);
-    case 16: return pick_for_h<16>(S);
-    default: return pick_for_h<0>(S);
+    case 10: return pick_for_h<10, FAST>(S);
+    case 11: return pick_for_h<11, FAST>(S);
+    case 16: return pick_for_h<16, FAST>(S);
+    default: return pick_for_h<0, FAST>(S);
   }
+}
+
+// fast: BF16 intensity storage with the fast f32 arithmetic (ADS_PRECISION_BF16)
+void (*pick_search_kernel(int h, int S, bool fast))(SearchArgs) {
+  return fast ? pick_for_precision<true>(h, S) : pick_for_precision<false>(h, S);
 }
 
 // ------------------------------------------------------------ compaction
@@ -433,6 +481,7 @@ struct AdsSelection {
   ads::DevBuf<uint32_t> blo, bhi;
   ads::DevBuf<uint8_t> keep;
   ads::DevBuf<unsigned long long> work;
+  ads::DevBuf<int> class_lists;
   ads::DevBuf<int64_t> block_sums;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // one set of four events per timed search since the last read-out
@@ -502,6 +551,59 @@ int64_t max_cycle_span(const std::vector<float>& rt, float delta_t, float tol, i
   return std::min<int64_t>(n, best + 4);
 }
 
+// Sorts the precursors into length classes: class b holds those with
+// bound[b-1] < C <= bound[b] (C = stop - start cycles), searched by a kernel
+// instance whose lanes cover the class's longest window.  Precursors with nothing
+// to search get no candidates here.  Order inside a class is arbitrary; results do
+// not depend on it.
+__global__ void classify_kernel(int64_t P, const int* nf, const int* cs, const int* ce, int n_cls,
+                                LenClasses cls, int* lists, unsigned int* counts, int* cand_n) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x; p0 < P; p0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = p0 + threadIdx.x;
+    int b = -1;
+    if (p < P) {
+      const int C = ce[p] - cs[p];
+      if (nf[p] == 0 || C <= 0) {
+        cand_n[p] = 0;
+      } else {
+        b = n_cls - 1;
+        for (int i = 0; i < n_cls - 1; ++i)
+          if (C <= cls.bound[i]) {
+            b = i;
+            break;
+          }
+      }
+    }
+    // one atomic per class present in the warp
+    const unsigned grp = __match_any_sync(kFull, b);
+    const int leader = __ffs(grp) - 1;
+    unsigned base = 0;
+    if (b >= 0 && lane == leader) base = atomicAdd(counts + b, (unsigned)__popc(grp));
+    base = __shfl_sync(kFull, base, leader);
+    if (b >= 0) lists[(int64_t)b * P + base + __popc(grp & ((1u << lane) - 1u))] = (int)p;
+  }
+}
+
+__global__ void to_bf16_kernel(int64_t n, const float* __restrict__ in, uint16_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = __bfloat16_as_ushort(__float2bfloat16_rn(in[i]));
+}
+
+// The bfloat16 copy of a run's intensities (round to nearest even), made on the
+// first BF16-storage search of that run and kept with it.
+int ensure_bf16_intensities(AdsDia* d, cudaStream_t st) {
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (d->intens_bf16.p || d->n_entries == 0) return ADS_OK;
+  ADS_TRY(d->intens_bf16.alloc((size_t)d->n_entries));
+  to_bf16_kernel<<<1184, 256, 0, st>>>(d->n_entries, d->intens.p, d->intens_bf16.p);
+  ADS_LAUNCH_CHECK();
+  // searches on other streams may read the copy next
+  ADS_CUDA(cudaStreamSynchronize(st));
+  return ADS_OK;
+}
+
 int reserve_candidates(AdsCandidates* c, int64_t cap) {
   if (c->cap >= cap) return ADS_OK;
   const size_t n = (size_t)std::max<int64_t>(cap, 1);
@@ -543,22 +645,15 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   if (c_max > kMaxCycles)
     return fail(ADS_ERR_INVALID_ARGUMENT, "RT windows longer than 2048 cycles are not supported (" +
                                               std::to_string(c_max) + " cycles)");
-  // cycles per lane: the fewest lane slots (passes * 32 * S) covering c_max, ties to
-  // the larger S
-  int S = s->o.cycles_per_lane;
-  if (S == 0) {
-    int64_t best = -1;
-    for (int cand : kLaneCycles) {
-      const int64_t slots = (c_max + 32 * cand - 1) / (32 * cand) * 32 * cand;
-      if (best < 0 || slots <= best) {
-        best = slots;
-        S = cand;
-      }
-    }
-  }
-  if (std::find(std::begin(kLaneCycles), std::end(kLaneCycles), S) == std::end(kLaneCycles))
+  // length classes and their cycles per lane (a fixed cycles_per_lane: one class)
+  const int S_fixed = s->o.cycles_per_lane;
+  if (S_fixed != 0 &&
+      std::find(std::begin(kLaneCycles), std::end(kLaneCycles), S_fixed) == std::end(kLaneCycles))
     return fail(ADS_ERR_INVALID_ARGUMENT, "cycles_per_lane must be 0 or one of 4, 8, 10, 13, 16");
-  const int ncell = (int)((c_max + 32 * S - 1) / (32 * S) * 32 * S);
+  LenClasses cls;
+  const int n_cls = plan_classes(c_max, S_fixed, &cls);
+  const int S_last = cls.S[n_cls - 1];
+  const int ncell = (int)((c_max + 32 * S_last - 1) / (32 * S_last) * 32 * S_last);
   const int k_out = (int)std::max<int64_t>(0, std::min<int64_t>(prm.candidate_count, maxima_cap(ncell)));
   const int kf = (int)std::max<int64_t>(1, std::min<int64_t>(prm.top_k_fragments, l->max_frag));
   const int maxw = std::max(1, d->max_overlap);
@@ -590,7 +685,8 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   ADS_TRY(s->cand_n.reserve(Pn));
   ADS_TRY(s->cand_score.reserve(Pn * k_out));
   ADS_TRY(s->cand_center.reserve(Pn * k_out));
-  ADS_TRY(s->work.reserve(1));
+  ADS_TRY(s->work.reserve(2 * kMaxClasses));  // work counters, then class lengths
+  if (n_cls > 1) ADS_TRY(s->class_lists.reserve(Pn * n_cls));
   const int64_t nb = (P + kScanBlock - 1) / kScanBlock;
   ADS_TRY(s->block_sums.reserve((size_t)nb));
   if (s->stats_on) {
@@ -636,7 +732,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   pa.blo = s->blo.p;
   pa.bhi = s->bhi.p;
   pa.err = c->err_p;
-  ADS_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned long long), st));
+  ADS_CUDA(cudaMemsetAsync(s->work.p, 0, 2 * kMaxClasses * sizeof(unsigned long long), st));
   const bool timed = s->o.time_stages != 0 && s->stage_used < 65536;
   if (timed) {
     if (s->stage_used == s->stage_pool.size()) {
@@ -653,24 +749,12 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
     ++launches;
   }
 
-  // block shape: warps per block (one precursor per warp at a time)
-  int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : 8;
-  nw = std::max(1, std::min(nw, 8));
-  int max_smem = 0;
-  ADS_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
-  while (nw > 1 && search_smem_bytes(nw, S, s->h, ncell) > (size_t)max_smem) --nw;
-  const size_t smem = search_smem_bytes(nw, S, s->h, ncell);
-  if (smem > (size_t)max_smem)
-    return fail(ADS_ERR_INVALID_ARGUMENT, "RT window too long for shared memory (" +
-                                              std::to_string(c_max) + " cycles)");
   const double2* ln_tab = nullptr;
   ADS_TRY(device_ln_table(s->device, &ln_tab));
-  void (*kern)(SearchArgs) = pick_search_kernel(s->h, S);
-  ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int occ = 0;
-  ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
-  if (occ <= 0) return fail(ADS_ERR_INTERNAL, "search kernel cannot be resident");
-  int bps = s->o.blocks_per_sm > 0 ? std::min(s->o.blocks_per_sm, occ) : occ;
+  const bool bf16 = s->o.precision == ADS_PRECISION_BF16;
+  if (bf16) ADS_TRY(ensure_bf16_intensities(const_cast<AdsDia*>(d), st));
+  int max_smem = 0;
+  ADS_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
 
   SearchArgs sa;
   std::memset(&sa, 0, sizeof(sa));
@@ -689,22 +773,50 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   sa.ss = d->slice_starts.p;
   sa.cyc = d->cycles.p;
   sa.inten = d->intens.p;
+  sa.inten_bf16 = d->intens_bf16.p;
   sa.ln_tab = ln_tab;
   for (int k = 0; k <= s->h; ++k) sa.kw[k] = s->kernel[k];
   sa.h = s->h;
   sa.k_out = k_out;
-  sa.c_max = (int)c_max;
-  sa.ncell = ncell;
   sa.gather_mode = s->o.gather_mode;
   sa.scan_thresh = 4 * 32 * kPrefetchChunks;
-  sa.work = s->work.p;
   sa.err = c->err_p;
   sa.cand_n = s->cand_n.p;
   sa.cand_score = s->cand_score.p;
   sa.cand_center = s->cand_center.p;
   sa.stats = s->stats_on ? s->stats.p : nullptr;
   if (timed) ADS_CUDA(cudaEventRecord(s->stage_ev[1], st));
-  {
+  unsigned int* class_len = reinterpret_cast<unsigned int*>(s->work.p + kMaxClasses);
+  if (n_cls > 1) {
+    const int cb = (int)std::min<int64_t>((P + 255) / 256, (int64_t)s->num_sms * 8);
+    classify_kernel<<<cb, 256, 0, st>>>(P, s->nf.p, s->cs.p, s->ce.p, n_cls, cls,
+                                         s->class_lists.p, class_len, s->cand_n.p);
+    ADS_LAUNCH_CHECK();
+    ++launches;
+  }
+  for (int b = 0; b < n_cls; ++b) {
+    const int S = cls.S[b];
+    const int cmax_b = cls.bound[b];
+    const int ncell_b = (cmax_b + 32 * S - 1) / (32 * S) * 32 * S;
+    // block shape: warps per block (one precursor per warp at a time)
+    int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : 8;
+    nw = std::max(1, std::min(nw, 8));
+    while (nw > 1 && search_smem_bytes(nw, S, s->h, ncell_b) > (size_t)max_smem) --nw;
+    const size_t smem = search_smem_bytes(nw, S, s->h, ncell_b);
+    if (smem > (size_t)max_smem)
+      return fail(ADS_ERR_INVALID_ARGUMENT, "RT window too long for shared memory (" +
+                                                std::to_string(c_max) + " cycles)");
+    void (*kern)(SearchArgs) = pick_search_kernel(s->h, S, bf16);
+    ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
+    if (occ <= 0) return fail(ADS_ERR_INTERNAL, "search kernel cannot be resident");
+    const int bps = s->o.blocks_per_sm > 0 ? std::min(s->o.blocks_per_sm, occ) : occ;
+    sa.list = n_cls > 1 ? s->class_lists.p + (int64_t)b * P : nullptr;
+    sa.list_len = n_cls > 1 ? class_len + b : nullptr;
+    sa.c_max = cmax_b;
+    sa.ncell = ncell_b;
+    sa.work = s->work.p + b;
     const int64_t blocks = std::min<int64_t>((int64_t)s->num_sms * bps, (P + nw - 1) / nw);
     kern<<<(int)blocks, nw * 32, smem, st>>>(sa);
     ADS_LAUNCH_CHECK();
@@ -808,8 +920,8 @@ int ads_selection_create(const AdsSelectionParams* params, const AdsEngineOption
       s->o = *options;
     else
       ads_engine_options_default(&s->o);
-    if (s->o.precision != ADS_PRECISION_FP32)
-      return fail(ADS_ERR_INVALID_ARGUMENT, "only ADS_PRECISION_FP32 is implemented");
+    if (s->o.precision != ADS_PRECISION_FP32 && s->o.precision != ADS_PRECISION_BF16)
+      return fail(ADS_ERR_INVALID_ARGUMENT, "precision must be ADS_PRECISION_FP32 or _BF16");
     if (s->o.gather_mode < 0 || s->o.gather_mode > 2)
       return fail(ADS_ERR_INVALID_ARGUMENT, "gather_mode must be 0, 1 or 2");
     ADS_TRY(check_params(s->p, &s->kernel, &s->h));
@@ -1176,7 +1288,7 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   if (smem > (size_t)max_smem)
     return fail(ADS_ERR_INVALID_ARGUMENT, "RT window too long for shared memory (" +
                                               std::to_string(c_max) + " cycles)");
-  void (*kern)(SearchArgs) = pick_search_kernel(h, S);
+  void (*kern)(SearchArgs) = pick_search_kernel(h, S, false);
   ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));

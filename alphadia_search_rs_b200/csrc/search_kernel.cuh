@@ -20,6 +20,8 @@
 
 struct SearchArgs {
   int64_t n_prec;
+  const int* list;                // nullable: the precursors to search, else 0..n_prec-1
+  const unsigned int* list_len;   // device length of `list`
   const int* nf;
   const int* cs;
   const int* ce;
@@ -34,11 +36,12 @@ struct SearchArgs {
   const uint32_t* ss;
   const uint16_t* cyc;
   const float* inten;
+  const uint16_t* inten_bf16;  // bfloat16 copy of `inten` (BF16-storage searches)
   const double2* ln_tab;
   float kw[kMaxHalf + 1];  // kernel taps w[0..h]; w[h] is the centre
   int h;
   int k_out;   // candidates kept per precursor
-  int c_max;   // largest cycle range any precursor can have
+  int c_max;   // largest cycle range of the precursors this launch searches
   int ncell;   // cycles a warp's row holds: passes * 32 * S >= c_max
   int gather_mode;
   int scan_thresh;
@@ -73,7 +76,7 @@ __host__ __device__ constexpr int floordiv(int a, int b) {
 // Per-warp shared-memory plan, in 4-byte words.  The block's ln table (double2 x
 // 256 = 1024 words) and kernel taps (32 words) come first.
 struct WarpPlan {
-  int row, tags, bm, scr, score, mval, midx, total;
+  int row, tags, bm, scr, score, cvb, mval, midx, total;
   int off;        // stored index of cycle c is c + off (off >= h, a multiple of S)
   int row_words;  // words of the row, a multiple of 4
   int bw;         // bitmap words
@@ -98,6 +101,8 @@ __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
   o += 32;
   w.score = o + 4;  // 4 words of margin below: the maxima scan reads 2 cycles early
   o += ncell + ncell / S + 12;
+  w.cvb = o;  // one pass of convolved values, lane l at l * (S + 1)
+  o += 32 * (S + 1);
   w.mx = maxima_cap(ncell);
   w.mval = o;
   o += w.mx;
@@ -114,6 +119,29 @@ __host__ __device__ inline size_t search_smem_bytes(int nw, int S, int h, int nc
 struct Counters {
   unsigned long long read = 0, acc = 0, off = 0, pairs = 0, bins1 = 0, frag = 0;
 };
+
+// The rare case of add_chunk: lanes that hit the same cycle are grouped and summed
+// by their lowest lane in lane order (kept out of line: it is seldom taken).
+static __device__ __noinline__ void add_chunk_grouped(bool inc, int cell, int addr, float v,
+                                                      int lane, float* row, uint32_t* bm,
+                                                      float* scr) {
+  const int key = inc ? cell : (-1 - lane);
+  const unsigned grp = __match_any_sync(kFull, key);
+  scr[lane] = v;
+  __syncwarp();
+  if (inc && lane == __ffs(grp) - 1) {
+    float acc = row[addr];
+    unsigned g = grp;
+    while (g) {
+      const int l = __ffs(g) - 1;
+      acc = __fadd_rn(acc, scr[l]);
+      g &= g - 1;
+    }
+    row[addr] = acc;
+    const int bit = cell + kBitOff;
+    atomicOr(bm + (bit >> 5), 1u << (bit & 31));
+  }
+}
 
 // Adds one chunk of 32 CSR-consecutive entries to the XIC row in lane order (the
 // reference's `dense_xic[c] += intensity`, src/quadrupole_observation/mod.rs:96-105).
@@ -139,21 +167,7 @@ __device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v,
       atomicOr(bm + (bit >> 5), 1u << (bit & 31));
     }
   } else {
-    const int key = inc ? cell : (-1 - lane);
-    const unsigned grp = __match_any_sync(kFull, key);
-    scr[lane] = v;
-    __syncwarp();
-    if (inc && lane == __ffs(grp) - 1) {
-      float acc = row[addr];
-      unsigned g = grp;
-      while (g) {
-        const int l = __ffs(g) - 1;
-        acc = __fadd_rn(acc, scr[l]);
-        g &= g - 1;
-      }
-      row[addr] = acc;
-      atomicOr(bm + (bit >> 5), 1u << (bit & 31));
-    }
+    add_chunk_grouped(inc, cell, addr, v, lane, row, bm, scr);
   }
   __syncwarp();
 }
@@ -179,27 +193,51 @@ __device__ __forceinline__ bool bin_starts_at(const uint32_t* ssw, uint32_t b0, 
 //            lands, src/quadrupole_observation/mod.rs:91-94);
 //   bsearch  per bin, binary-search the first kept entry and the first entry at or
 //            past stop, then read only the kept entries.
-template <int S>
-__device__ void gather_pair(const SearchArgs& a, const WinInfo& wi, uint32_t b0, uint32_t b1,
-                            int64_t rs, int64_t re, int cs, int ce, int lane, float* row, int off,
-                            uint32_t* bm, uint32_t* tags, float* scr, uint32_t& seq, Counters& k) {
+// Up to 32 * kPrefetchChunks CSR entries (cycle, intensity) of a scanned range,
+// one per lane and chunk, -1 / 0 past its end.
+struct ScanBatch {
+  int c[kPrefetchChunks];
+  float v[kPrefetchChunks];
+};
+
+// Intensity of CSR entry i: f32, or (BF16 storage) the bfloat16 copy widened.
+template <bool FAST>
+__device__ __forceinline__ float ld_intensity(const SearchArgs& a, int64_t i) {
+  if (FAST) return __uint_as_float((uint32_t)__ldg(a.inten_bf16 + i) << 16);
+  return __ldg(a.inten + i);
+}
+
+template <bool FAST>
+__device__ __forceinline__ void load_batch(const SearchArgs& a, int64_t wbase, int64_t q0,
+                                           int64_t re, int lane, ScanBatch& b) {
+#pragma unroll
+  for (int u = 0; u < kPrefetchChunks; ++u) {
+    const int64_t q = q0 + u * 32 + lane;
+    b.c[u] = q < re ? (int)__ldg(a.cyc + wbase + q) : -1;
+    b.v[u] = q < re ? ld_intensity<FAST>(a, wbase + q) : 0.0f;
+  }
+}
+
+__device__ __forceinline__ bool scans(const SearchArgs& a, int64_t n) {
+  return a.gather_mode == 1 || (a.gather_mode == 0 && n <= a.scan_thresh);
+}
+
+template <int S, bool FAST>
+__device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64_t wbase,
+                                            uint32_t b0, uint32_t b1, int64_t rs, int64_t re,
+                                            int cs, int ce, int lane, float* row, int off,
+                                            uint32_t* bm, uint32_t* tags, float* scr,
+                                            uint32_t& seq, Counters& k) {
   const int64_t n = re - rs;
   if (n <= 0) return;
-  const uint32_t* ssw = a.ss + wi.ss_off;
-  const uint16_t* cy = a.cyc + wi.base;
-  const float* in = a.inten + wi.base;
-  const bool scan = a.gather_mode == 1 || (a.gather_mode == 0 && n <= a.scan_thresh);
-  if (scan) {
+  const uint16_t* cy = a.cyc + wbase;
+  if (scans(a, n)) {
     k.read += n;
     for (int64_t q0 = rs; q0 < re; q0 += 32 * kPrefetchChunks) {
-      int c[kPrefetchChunks];
-      float v[kPrefetchChunks];
-#pragma unroll
-      for (int u = 0; u < kPrefetchChunks; ++u) {
-        const int64_t q = q0 + u * 32 + lane;
-        c[u] = q < re ? (int)__ldg(cy + q) : -1;
-        v[u] = q < re ? __ldg(in + q) : 0.0f;
-      }
+      ScanBatch bt;
+      load_batch<FAST>(a, wbase, q0, re, lane, bt);
+      const int* c = bt.c;
+      const float* v = bt.v;
 #pragma unroll
       for (int u = 0; u < kPrefetchChunks; ++u) {
         const int64_t qb = q0 + u * 32;
@@ -213,7 +251,7 @@ __device__ void gather_pair(const SearchArgs& a, const WinInfo& wi, uint32_t b0,
         if (q < re && cu == cs) {
           const int64_t qn = q + 1;
           bool last = qn >= re;
-          if (!last) last = bin_starts_at(ssw, b0, b1, qn);
+          if (!last) last = bin_starts_at(a.ss + a.win[wsel].ss_off, b0, b1, qn);
           if (!last) {
             const int cn = nxt == -2 ? (int)__ldg(cy + qn) : nxt;
             last = cn != cs;
@@ -226,6 +264,7 @@ __device__ void gather_pair(const SearchArgs& a, const WinInfo& wi, uint32_t b0,
       }
     }
   } else {
+    const uint32_t* ssw = a.ss + a.win[wsel].ss_off;
     for (uint32_t bb = b0; bb < b1; bb += 32) {
       const uint32_t b = bb + lane;
       const bool vb = b < b1;
@@ -260,7 +299,7 @@ __device__ void gather_pair(const SearchArgs& a, const WinInfo& wi, uint32_t b0,
         const bool vt = t < total;
         const int64_t q = opos + (t - oex);
         const int c = vt ? (int)__ldg(cy + q) : 0;
-        const float v = vt ? __ldg(in + q) : 0.0f;
+        const float v = vt ? ld_intensity<FAST>(a, wbase + q) : 0.0f;
         const int cell = c - cs;
         add_chunk(vt, cell, vt ? xaddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, seq, k.acc);
       }
@@ -284,24 +323,84 @@ __device__ __forceinline__ bool bits_any(const uint32_t* bm, int lo, int n) {
 
 // One output of convolution_scalar (src/convolution/scalar.rs:30-50) read from the
 // row in shared memory: x[j]*w[h] first, then (x[j-d] + x[j+d]) * w[h-d] for
-// d = h..1.  Any half width; used off the main path.
-template <int S>
+// d = h..1.  Any half width; used off the main path.  FAST (BF16 storage) fuses
+// each multiply-add.
+template <int S, bool FAST>
 __device__ __forceinline__ float conv_at(const float* row, int off, const float* kw_s, int h,
                                          int j) {
   float s = __fadd_rn(0.0f, __fmul_rn(row[xaddr<S>(j + off)], kw_s[h]));
-  for (int t = 0; t < h; ++t)
-    s = __fadd_rn(s, __fmul_rn(__fadd_rn(row[xaddr<S>(j - h + t + off)], row[xaddr<S>(j + h - t + off)]),
-                              kw_s[t]));
+  for (int t = 0; t < h; ++t) {
+    const float lr = __fadd_rn(row[xaddr<S>(j - h + t + off)], row[xaddr<S>(j + h - t + off)]);
+    s = FAST ? __fmaf_rn(lr, kw_s[t], s) : __fadd_rn(s, __fmul_rn(lr, kw_s[t]));
+  }
   return s;
 }
 
-// score[j] += ln(c + 1) * w, one rounded operation at a time (src/score/scalar.rs:16-22).
-__device__ __forceinline__ void score_add(float* score, int addr, float c, float w,
-                                          const double2* lnt) {
-  score[addr] = __fadd_rn(score[addr], __fmul_rn(ln_fast(__fadd_rn(c, 1.0f), lnt), w));
+// ln(1 + c) for the BF16-storage path: the hardware log2 (absolute error about
+// 2^-21) where ln(1 + c) >= ln(17/16), and the series c - c^2/2 + ... + c^7/7
+// (relative error below 2^-26) for |c| < 1/16, so that small terms keep their
+// relative accuracy.
+__device__ __forceinline__ float ln1p_fast(float c) {
+  float p = __fmaf_rn(c, -1.0f / 7.0f, 1.0f / 6.0f);
+  p = __fmaf_rn(c, p, -1.0f / 5.0f);
+  p = __fmaf_rn(c, p, 1.0f / 4.0f);
+  p = __fmaf_rn(c, p, -1.0f / 3.0f);
+  p = __fmaf_rn(c, p, 1.0f / 2.0f);
+  p = __fmaf_rn(c, -p, 1.0f);  // 1 - c/2 + c^2/3 - ...
+  const float series = __fmul_rn(c, p);
+  return fabsf(c) < 0.0625f ? series : __logf(__fadd_rn(c, 1.0f));
 }
 
-template <int H, int S>
+// score[j] += ln(c + 1) * w (src/score/scalar.rs:16-22): one rounded operation at a
+// time with the exact ln; FAST (BF16 storage) takes the hardware log2 and a fused
+// multiply-add.
+template <bool FAST>
+__device__ __forceinline__ float score_term(float s, float c, float w, const double2* lnt) {
+  if (FAST) return __fmaf_rn(ln1p_fast(c), w, s);
+  return __fadd_rn(s, __fmul_rn(ln_fast(__fadd_rn(c, 1.0f), lnt), w));
+}
+
+template <bool FAST>
+__device__ __forceinline__ void score_add(float* score, int addr, float c, float w,
+                                          const double2* lnt) {
+  if (FAST)
+    score[addr] = __fmaf_rn(ln1p_fast(c), w, score[addr]);
+  else
+    score[addr] = __fadd_rn(score[addr], __fmul_rn(ln_fast(__fadd_rn(c, 1.0f), lnt), w));
+}
+
+// Candidate order: value descending, then cycle ascending (maxima values are never
+// NaN: every comparison with NaN is false, so NaN is never a strict maximum).
+__device__ __forceinline__ bool better(float av, int ai, float bv, int bi) {
+  return av > bv || (av == bv && ai < bi);
+}
+
+// Compare-exchange between lanes l and l ^ j, the better key going to the lane
+// that `keep_best` marks.
+__device__ __forceinline__ void cmpx(float& v, int& i, int j, bool keep_best) {
+  const float ov = __shfl_xor_sync(kFull, v, j);
+  const int oi = __shfl_xor_sync(kFull, i, j);
+  if (keep_best ? better(ov, oi, v, i) : better(v, i, ov, oi)) {
+    v = ov;
+    i = oi;
+  }
+}
+
+// Bitonic sort of one key per lane, best in lane 0.
+__device__ __forceinline__ void warp_sort_best_first(float& v, int& i, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) cmpx(v, i, j, ((lane & j) == 0) == ((lane & k) == 0));
+}
+
+// Sorts a bitonic sequence across the lanes, best in lane 0.
+__device__ __forceinline__ void warp_merge_best_first(float& v, int& i, int lane) {
+#pragma unroll
+  for (int j = 16; j > 0; j >>= 1) cmpx(v, i, j, (lane & j) == 0);
+}
+
+template <int H, int S, bool FAST>
 __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
   extern __shared__ __align__(16) float smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -315,6 +414,7 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
   uint32_t* bm = reinterpret_cast<uint32_t*>(wb + P.bm);
   float* scr = wb + P.scr;
   float* score = wb + P.score;
+  float* cvb = wb + P.cvb + lane * (S + 1);
   float* mval = wb + P.mval;
   int* midx = reinterpret_cast<int*>(wb + P.midx);
 
@@ -325,12 +425,14 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
   Counters k;
   uint32_t seq = 1;
 
+  const unsigned long long n_work = a.list ? (unsigned long long)*a.list_len
+                                            : (unsigned long long)a.n_prec;
   for (;;) {
     unsigned long long pw = 0;
     if (lane == 0) pw = atomicAdd(a.work, 1ull);
     pw = __shfl_sync(kFull, pw, 0);
-    if (pw >= (unsigned long long)a.n_prec) break;
-    const int64_t p = (int64_t)pw;
+    if (pw >= n_work) break;
+    const int64_t p = a.list ? (int64_t)a.list[pw] : (int64_t)pw;
     const int F = a.nf[p];
     const int cs = a.cs[p], ce = a.ce[p];
     const int C = ce - cs;
@@ -356,11 +458,12 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
       seq = 1;
     }
 
-    // CSR offsets of up to 32 (fragment, window) pairs, fetched together
+    // CSR ranges of up to 32 (fragment, window) pairs, fetched together: lane q
+    // holds pair pb + q
     int pb = -64;
-    int64_t rs = 0, re = 0;
-    uint32_t b0 = 0, b1 = 0;
+    uint32_t rs = 0, re = 0, b0 = 0, b1 = 0;
     int wsel = 0;
+    int64_t wbase = 0;
     for (int f = 0; f < F; ++f) {
       {
         float4* r4 = reinterpret_cast<float4*>(row);
@@ -378,6 +481,7 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
           rs = re = 0;
           b0 = b1 = 0;
           wsel = 0;
+          wbase = 0;
           if (pj < npairs) {
             const int fj = pj / nwin, wj = pj - fj * nwin;
             const int64_t fo = p * a.kf + fj;
@@ -386,23 +490,25 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
             wsel = a.wins[p * a.maxw + wj];
             if (b1 > b0) {
               const WinInfo w = a.win[wsel];
+              wbase = w.base;
               rs = __ldg(a.ss + w.ss_off + b0);
               re = __ldg(a.ss + w.ss_off + b1);
             }
           }
         }
         const int q = pi - pb;
-        const int64_t qrs = __shfl_sync(kFull, rs, q);
-        const int64_t qre = __shfl_sync(kFull, re, q);
+        const uint32_t qrs = __shfl_sync(kFull, rs, q);
+        const uint32_t qre = __shfl_sync(kFull, re, q);
         const uint32_t qb0 = __shfl_sync(kFull, b0, q);
         const uint32_t qb1 = __shfl_sync(kFull, b1, q);
         const int qw = __shfl_sync(kFull, wsel, q);
+        const int64_t qbase = __shfl_sync(kFull, wbase, q);
         if (qb1 <= qb0) continue;
-        const WinInfo w = a.win[qw];
         k.off += 2;
         k.pairs += 1;
         k.bins1 += qb1 - qb0 + 1;
-        gather_pair<S>(a, w, qb0, qb1, qrs, qre, cs, ce, lane, row, P.off, bm, tags, scr, seq, k);
+        gather_pair<S, FAST>(a, qw, qbase, qb0, qb1, qrs, qre, cs, ce, lane, row, P.off, bm, tags,
+                             scr, seq, k);
       }
       __syncwarp();
       const float wf = __ldg(a.fw + p * a.kf + f);
@@ -410,8 +516,8 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
         // ln(conv + 1) * inf is NaN even where conv is zero: every column takes
         // its term, as in the reference
         for (int j = lane; j < C; j += 32) {
-          const float c = (j >= h && j < C - h) ? conv_at<S>(row, P.off, kw_s, h, j) : 0.0f;
-          score_add(score, xaddr<S>(j), c, wf, lnt);
+          const float c = (j >= h && j < C - h) ? conv_at<S, FAST>(row, P.off, kw_s, h, j) : 0.0f;
+          score_add<FAST>(score, xaddr<S>(j), c, wf, lnt);
         }
         __syncwarp();
         continue;
@@ -430,21 +536,37 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
           float x[S + 2 * H];
 #pragma unroll
           for (int t = 0; t < S + 2 * H; ++t) x[t] = rb[(t - H) + floordiv(t - H, S)];
+          // each output in the reference's order: 0 + x[j]*w[h], then
+          // + (x[j-d] + x[j+d]) * w[h-d] for d = h..1; parked in this lane's cvb
+          // slots so that the log below exists once in the code
 #pragma unroll
           for (int m = 0; m < S; ++m) {
-            const int j = j0 + m;
             float s = __fadd_rn(0.0f, __fmul_rn(x[m + H], a.kw[H]));
 #pragma unroll
-            for (int t = 0; t < H; ++t)
-              s = __fadd_rn(s, __fmul_rn(__fadd_rn(x[m + t], x[m + 2 * H - t]), a.kw[t]));
-            if (s != 0.0f && j >= H && j < C - H) score_add(sb, m, s, wf, lnt);
+            for (int t = 0; t < H; ++t) {
+              const float lr = __fadd_rn(x[m + t], x[m + 2 * H - t]);
+              s = FAST ? __fmaf_rn(lr, a.kw[t], s) : __fadd_rn(s, __fmul_rn(lr, a.kw[t]));
+            }
+            cvb[m] = s;
           }
+          // score terms of the valid outputs [m0, m1), two at a time; a zero output
+          // adds ln(1) * w = +0, which leaves the score as it is
+          const int m0 = max(H - j0, 0), m1 = min(C - H - j0, S);
+          int m = m0;
+#pragma unroll 1
+          for (; m + 1 < m1; m += 2) {
+            const float c0 = cvb[m], c1 = cvb[m + 1];
+            const float s0 = sb[m], s1 = sb[m + 1];
+            sb[m] = score_term<FAST>(s0, c0, wf, lnt);
+            sb[m + 1] = score_term<FAST>(s1, c1, wf, lnt);
+          }
+          if (m < m1) sb[m] = score_term<FAST>(sb[m], cvb[m], wf, lnt);
         } else {
           for (int m = 0; m < S; ++m) {
             const int j = j0 + m;
             if (j < h || j >= C - h) continue;
-            const float s = conv_at<S>(row, P.off, kw_s, h, j);
-            if (s != 0.0f) score_add(score, xaddr<S>(j), s, wf, lnt);
+            const float s = conv_at<S, FAST>(row, P.off, kw_s, h, j);
+            if (s != 0.0f) score_add<FAST>(score, xaddr<S>(j), s, wf, lnt);
           }
         }
       }
@@ -498,7 +620,34 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
     // top-K by (value descending, cycle ascending): the reference's stable sort by
     // value of maxima found in cycle order (src/peak_group_selection/mod.rs:45-61).
     const int kk = min(a.k_out, nmax);
-    for (int r = 0; r < kk; ++r) {
+    if (a.k_out <= 32) {
+      // the best 32 of the maxima, sorted in the lanes: chunks of 32 are sorted
+      // and merged into the running best 32
+      float bv = -INFINITY;
+      int bi = INT_MAX;
+      for (int q0 = 0; q0 < nmax; q0 += 32) {
+        float v = q0 + lane < nmax ? mval[q0 + lane] : -INFINITY;
+        int i = q0 + lane < nmax ? midx[q0 + lane] : INT_MAX;
+        warp_sort_best_first(v, i, lane);
+        if (q0 == 0) {
+          bv = v;
+          bi = i;
+        } else {
+          const float rv = __shfl_sync(kFull, v, 31 - lane);
+          const int ri = __shfl_sync(kFull, i, 31 - lane);
+          if (better(rv, ri, bv, bi)) {
+            bv = rv;
+            bi = ri;
+          }
+          warp_merge_best_first(bv, bi, lane);
+        }
+      }
+      if (lane < kk) {
+        a.cand_score[p * a.k_out + lane] = bv;
+        a.cand_center[p * a.k_out + lane] = cs + bi;
+      }
+    }
+    for (int r = 0; a.k_out > 32 && r < kk; ++r) {
       float bv = 0.0f;
       int bi = -1, bk = -1;
       for (int q = lane; q < nmax; q += 32) {

@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--warps-per-block", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--cycles-per-lane", type=int, default=0)
+    ap.add_argument("--precision", choices=["fp32", "bf16"], default=None,
+                    help="override the workload's precision (cfg3/cfg4: bf16 storage)")
     return ap.parse_args()
 
 
@@ -363,7 +365,8 @@ def run_ours(args, rank, world, local_rank):
     params.update(cfg.params_dict())
 
     # counters pass (untimed): algorithmic bytes of the gather
-    sel_stats = ads.PeakGroupSelection(params, verbose=False, device=local_rank)
+    precision = args.precision or cfg.precision
+    sel_stats = ads.PeakGroupSelection(params, verbose=False, device=local_rank, precision=precision)
     sel_stats.enable_stats(True)
     cand_full = sel_stats.search(dia, slib)
     stats = sel_stats.last_stats()
@@ -382,6 +385,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.empty_cache()
 
     sel = ads.PeakGroupSelection(params, verbose=False, device=local_rank, time_stages=True,
+                                 precision=precision,
                                  warps_per_block=args.warps_per_block,
                                  cycles_per_lane=args.cycles_per_lane,
                                  blocks_per_sm=args.blocks_per_sm)
@@ -425,7 +429,7 @@ def run_ours(args, rank, world, local_rank):
     cap = max(n_cand, 1)
     out_t = [torch.empty(cap, dtype=torch.float32 if i == 2 else torch.uint64).pin_memory() for i in range(9)]
     out_np = tuple(t.numpy() for t in out_t)
-    sel_e2e = ads.PeakGroupSelection(params, verbose=False, device=local_rank)
+    sel_e2e = ads.PeakGroupSelection(params, verbose=False, device=local_rank, precision=precision)
     h2d = sum(lib_np[k].nbytes for k in ("precursor_idx", "precursor_mz", "precursor_rt",
                                           "flat_frag_start_idx", "flat_frag_stop_idx", "fragment_mz",
                                           "fragment_intensity", "fragment_number", "fragment_type"))
@@ -458,7 +462,7 @@ def run_ours(args, rank, world, local_rank):
     search_ms = st["search_ms"] / n_searches
     prep_ms = st["prep_ms"] / n_searches
     comp_ms = st["compaction_ms"] / n_searches
-    s_i = 4  # f32 intensities
+    s_i = 2 if precision == "bf16" else 4  # bytes per stored intensity
     gather_bytes = 4 * stats["bins_plus_one"] + (2 + s_i) * stats["entries_accumulated"]
     path_bytes = 8 * P + 8 * nf_raw + gather_bytes + 68 * n_cand
     peak, peak_kind = measured_peak()
@@ -511,7 +515,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"{cfg.name}: {cfg.n_cycles} cycles x {cfg.n_windows} MS2 windows of "
                                f"{cfg.window_width} Th, {cfg.peaks_per_spectrum} peaks/spectrum, "
                                f"{cfg.n_precursors} precursors x {cfg.frag_min}-{cfg.frag_max} fragments",
-                   "precision": "fp32", "params": cfg.params_dict(),
+                   "precision": precision, "params": cfg.params_dict(),
                    "l2": "inputs larger than L2 (resident run ~%.1f GB), no flush" %
                          (dia.memory_footprint_bytes() / 1e9),
                    "peaks": n_peaks_total, "candidates_per_step": int(n_cand),

@@ -1,0 +1,71 @@
+"""GPU: the BF16-storage search (peak intensities read as bfloat16, FP32 arithmetic
+with the hardware log2) against the FP64 oracle.
+
+Relative score error is taken against max(|s64|, 1e-3 * max |s64| of the
+precursor), because scores near zero are common at the RT-window edges.  Bounds:
+  * top-k candidate cycles: at least 99.5% identical to the oracle's (99% on the
+    few-hundred-precursor cases);
+  * scores: bfloat16 keeps 8 significant bits, so every stored intensity is within
+    u = 2^-8 relative; a convolved value of non-negative intensities is then within
+    u, each ln(c + 1) term within u (ln(1 + c) >= c / (1 + c)), and the score, a
+    positive-weighted sum of such terms, within u -- the test allows u plus f32
+    noise for the maximum, and 1e-3 for the 99th percentile.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from alphadia_search_rs_b200 import synth
+
+from _util import oracle_inputs, product_search
+
+pytestmark = pytest.mark.gpu
+
+BF16_U = 2.0 ** -8
+SCORE_MAX_BF16 = BF16_U * 1.01
+SCORE_P99_BF16 = 1e-3
+EPS_REL_MAX = 1e-3
+
+
+def compare_to_fp64(got: dict, ref: dict):
+    """(fraction of the oracle's (precursor, rank) rows with the same cycle, the
+    relative score errors over those rows)."""
+    ref_max = {}
+    for p, s in zip(ref["precursor_idx"], ref["score_f64"]):
+        ref_max[int(p)] = max(ref_max.get(int(p), 0.0), abs(float(s)))
+    mine = {(int(p), int(r)): (int(c), float(s)) for p, r, c, s in
+            zip(got["precursor_idx"], got["rank"], got["cycle_center"], got["score"])}
+    same, errs = 0, []
+    for p, r, c, s in zip(ref["precursor_idx"], ref["rank"], ref["cycle_center"], ref["score_f64"]):
+        m = mine.get((int(p), int(r)))
+        if m is None or m[0] != int(c):
+            continue
+        same += 1
+        den = max(abs(float(s)), EPS_REL_MAX * ref_max[int(p)])
+        errs.append(abs(m[1] - float(s)) / den if den > 0 else 0.0)
+    return same / max(len(ref["rank"]), 1), np.asarray(errs if errs else [0.0])
+
+
+@pytest.mark.parametrize("name,min_agree", [("tiny", 0.99), ("tiny_uneven", 0.99), ("cfg0", 0.995)])
+def test_bf16_against_fp64_oracle(name, min_agree):
+    cfg, lib, run = synth.make_workload(name, "numpy")
+    la = synth.library_arrays(lib)
+    got, *_ = product_search(run, la, cfg.params_dict(), precision="bf16")
+    od, ol, tol = oracle_inputs(run, la)
+    ref = oracle.search(od, ol, oracle.Params(**cfg.params_dict()), rt_tolerance_per_precursor=tol,
+                        log_mode=oracle.LOG_RN, precision=1)
+    assert len(ref["rank"]) > 0
+    agree, errs = compare_to_fp64(got, ref)
+    assert agree >= min_agree, f"{name}: top-k cycle agreement {agree:.4f}"
+    assert errs.max() <= SCORE_MAX_BF16, f"{name}: max relative score error {errs.max():.2e}"
+    p99 = float(np.quantile(errs, 0.99))
+    assert p99 <= SCORE_P99_BF16, f"{name}: 99th percentile relative score error {p99:.2e}"
+
+
+def test_bf16_deterministic():
+    cfg, lib, run = synth.make_workload("tiny_uneven", "numpy")
+    la = synth.library_arrays(lib)
+    a, *_ = product_search(run, la, cfg.params_dict(), precision="bf16")
+    b, *_ = product_search(run, la, cfg.params_dict(), precision="bf16", warps_per_block=2)
+    for k in a:
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
