@@ -129,6 +129,8 @@ SIGNATURES = {
     "ads_selection_kernel": (C.c_int, [vp, vp, i64, C.POINTER(i64)]),
     "ads_select": (C.c_int, [vp, vp, vp, C.POINTER(vp)]),
     "ads_select_async": (C.c_int, [vp, vp, vp, vp]),
+    "ads_selection_autotune": (C.c_int, [vp, vp, vp, i32, C.POINTER(i32), C.POINTER(i32),
+                                         C.POINTER(C.c_float)]),
     # allocation-free search: dia, lib, params*, stream, capacity, six device output
     # columns, device int64 count, device int32 flags (nullable)
     "ads_select_noalloc": (C.c_int, [vp, vp, C.POINTER(AdsSelectionParams), i64, i64,

@@ -450,7 +450,7 @@ class PeakGroupSelection:
     def __init__(self, params: SelectionParameters, *, precision: str = "fp32", verbose: bool = True,
                  device: int | None = None, warps_per_block: int = 0, blocks_per_sm: int = 0,
                  gather_mode: int = 0, time_stages: bool = False, stream: int = 0,
-                 cycles_per_lane: int = 0):
+                 cycles_per_lane: int = 0, use_graph: bool = False):
         if not isinstance(params, SelectionParameters):
             raise TypeError("argument 'params': expected SelectionParameters")
         L = _lib()
@@ -465,6 +465,7 @@ class PeakGroupSelection:
         o.gather_mode = gather_mode
         o.time_stages = 1 if time_stages else 0
         o.cycles_per_lane = int(cycles_per_lane)
+        o.use_graph = 1 if use_graph else 0
         o.stream = int(stream)
         self._opts = o
         p = params._c()
@@ -503,6 +504,14 @@ class PeakGroupSelection:
     def search_into(self, dia_data: DIAData, lib: SpecLibFlat, cand: "DeviceCandidates") -> None:
         """Enqueue a search without waiting, reusing ``cand``'s device buffers."""
         F.check(_lib().ads_select_async(self._h, dia_data._h, lib._h, cand._h))
+
+    def autotune(self, dia_data: DIAData, lib: SpecLibFlat, repeats: int = 2) -> dict:
+        """Times the launch shapes on this run and library and keeps the fastest
+        (cached per workload shape for the process); returns the choice."""
+        w, c, ms = C.c_int32(), C.c_int32(), C.c_float()
+        F.check(_lib().ads_selection_autotune(self._h, dia_data._h, lib._h, int(repeats),
+                                               C.byref(w), C.byref(c), C.byref(ms)))
+        return dict(warps_per_block=w.value, cycles_per_lane=c.value, ms=ms.value)
 
     def new_candidates(self) -> "DeviceCandidates":
         return DeviceCandidates(self)

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <memory>
 
 #include <cuda_bf16.h>
@@ -488,11 +489,16 @@ struct AdsSelection {
   std::vector<std::array<cudaEvent_t, 4>> stage_pool;
   size_t stage_used = 0;
   cudaEvent_t* stage_ev = nullptr;  // set of the search being enqueued
+  // use_graph: the pipeline captured for one (run, library, collection) and the
+  // buffers it was captured with
+  cudaGraphExec_t graph = nullptr;
+  std::vector<const void*> graph_key;
+  int64_t graph_launches = 0;
 };
 
 // A candidate collection does not depend on the selection that filled it: the
 // search records `done` on the selection's stream, and every later read waits on
-// that event from the collection's own copy stream.
+// that event from the calling thread's per-thread stream.
 struct AdsCandidates {
   int device = 0;
   cudaEvent_t done = nullptr;
@@ -622,14 +628,18 @@ int reserve_candidates(AdsCandidates* c, int64_t cap) {
   return ADS_OK;
 }
 
-int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidates* c) {
+// Enqueues one search on the selection's stream.  While `capturing` (stream
+// capture for a CUDA graph) it leaves out the cross-stream wait, the stage timing
+// and the completion record, which the graph's caller does around each replay.
+int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidates* c,
+                   bool capturing) {
   if (d->device != s->device || l->device != s->device || c->device != s->device)
     return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
   DeviceGuard dg(s->device);
   cudaStream_t st = s->o.stream ? (cudaStream_t)s->o.stream : s->stream;
   if (!c->done) {
     ADS_CUDA(cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming));
-  } else {
+  } else if (!capturing) {
     // a previous search into these buffers (possibly on another stream) comes first;
     // read-outs are synchronous, so none is in flight
     ADS_CUDA(cudaStreamWaitEvent(st, c->done, 0));
@@ -665,7 +675,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   c->count = 0;
   if (P == 0 || k_out == 0) {
     s->last_launches = 0;
-    ADS_CUDA(cudaEventRecord(c->done, st));
+    if (!capturing) ADS_CUDA(cudaEventRecord(c->done, st));
     return ADS_OK;
   }
 
@@ -733,7 +743,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   pa.bhi = s->bhi.p;
   pa.err = c->err_p;
   ADS_CUDA(cudaMemsetAsync(s->work.p, 0, 2 * kMaxClasses * sizeof(unsigned long long), st));
-  const bool timed = s->o.time_stages != 0 && s->stage_used < 65536;
+  const bool timed = !capturing && s->o.time_stages != 0 && s->stage_used < 65536;
   if (timed) {
     if (s->stage_used == s->stage_pool.size()) {
       std::array<cudaEvent_t, 4> set{};
@@ -852,7 +862,142 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
     ++s->stage_used;
   }
   s->last_launches = launches;
-  ADS_CUDA(cudaEventRecord(c->done, st));
+  if (!capturing) ADS_CUDA(cudaEventRecord(c->done, st));
+  return ADS_OK;
+}
+
+// ------------------------------------------------------------------ autotuner
+// Launch shapes of the search kernel: warps per block (precursors in flight per
+// CTA) and cycles per lane (0 = length classes, else one fixed width), timed on the
+// caller's run and library; the fastest is kept in the selection's options and
+// cached per workload shape for the rest of the process.
+struct TuneKey {
+  int device, precision, h;
+  int64_t c_max, P, kf, n_frag;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(device, precision, h, c_max, P, kf, n_frag) <
+           std::tie(o.device, o.precision, o.h, o.c_max, o.P, o.kf, o.n_frag);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::array<float, 3>> g_tune_cache;  // warps, cycles per lane, ms
+
+int autotune(AdsSelection* s, const AdsDia* d, const AdsLib* l, int32_t repeats,
+             int32_t* out_warps, int32_t* out_cycles, float* out_ms) {
+  if (!s || !d || !l) return fail(ADS_ERR_INVALID_ARGUMENT, "null argument");
+  if (d->device != s->device || l->device != s->device)
+    return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
+  repeats = std::max(1, std::min<int32_t>(repeats, 100));
+  const float tol_max = l->has_tol ? std::max(l->max_tol, 0.0f) : s->p.rt_tolerance;
+  const TuneKey key{s->device, s->o.precision, s->h,
+                    max_cycle_span(d->rt, d->delta_t, tol_max, s->p.kernel_size), l->n_prec,
+                    std::min<int64_t>(s->p.top_k_fragments, l->max_frag), l->n_frag};
+  std::array<float, 3> best{0.0f, 0.0f, -1.0f};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) best = it->second;
+  }
+  if (best[2] < 0.0f) {
+    DeviceGuard dg(s->device);
+    cudaStream_t st = s->o.stream ? (cudaStream_t)s->o.stream : s->stream;
+    struct Restore {  // the caller's options come back on every exit path
+      AdsSelection* s;
+      AdsEngineOptions o;
+      ~Restore() { s->o = o; }
+    } restore{s, s->o};
+    s->o.use_graph = 0;
+    s->o.time_stages = 0;
+    AdsCandidates scratch;
+    scratch.device = s->device;
+    int rc = ADS_OK;
+    for (int nw : {2, 4, 8}) {
+      for (int S : {0, 4, 8, 10, 13, 16}) {
+        if (S != 0 && (int64_t)32 * S * 8 < key.c_max) continue;  // more than 8 passes
+        s->o.warps_per_block = nw;
+        s->o.cycles_per_lane = S;
+        rc = enqueue_search(s, d, l, &scratch, false);  // warm-up (and buffer sizing)
+        float total = 0.0f;
+        for (int r = 0; rc == ADS_OK && r < repeats; ++r) {
+          ADS_CUDA(cudaEventRecord(s->ev0, st));
+          rc = enqueue_search(s, d, l, &scratch, false);
+          ADS_CUDA(cudaEventRecord(s->ev1, st));
+          ADS_CUDA(cudaEventSynchronize(s->ev1));
+          float ms = 0.0f;
+          ADS_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+          total += ms;
+        }
+        if (rc != ADS_OK) break;
+        const float ms = total / repeats;
+        if (best[2] < 0.0f || ms < best[2]) best = {(float)nw, (float)S, ms};
+      }
+      if (rc != ADS_OK) break;
+    }
+    ADS_CUDA(cudaStreamSynchronize(st));
+    if (rc != ADS_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  s->o.warps_per_block = (int32_t)best[0];
+  s->o.cycles_per_lane = (int32_t)best[1];
+  if (s->graph) {  // captured with the previous shape
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  if (out_warps) *out_warps = (int32_t)best[0];
+  if (out_cycles) *out_cycles = (int32_t)best[1];
+  if (out_ms) *out_ms = best[2];
+  return ADS_OK;
+}
+
+// Everything a captured search depends on: the handles and every buffer address.
+std::vector<const void*> graph_key(const AdsSelection* s, const AdsDia* d, const AdsLib* l,
+                                   const AdsCandidates* c) {
+  return {d, l, c, c->arena.p, s->nf.p, s->cs.p, s->ce.p, s->nwin.p, s->wins.p, s->fw.p,
+          s->blo.p, s->bhi.p, s->keep.p, s->cand_n.p, s->cand_score.p, s->cand_center.p,
+          s->work.p, s->class_lists.p, s->block_sums.p, s->stats_on ? s->stats.p : nullptr,
+          d->intens_bf16.p};
+}
+
+// A search, with use_graph: the first search of a (run, library, collection) runs
+// directly (sizing every buffer) and is then captured into a CUDA graph; later
+// searches with the same handles and buffers replay the graph in one launch.
+int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidates* c) {
+  if (!s->o.use_graph) return enqueue_search(s, d, l, c, false);
+  DeviceGuard dg(s->device);
+  cudaStream_t st = s->o.stream ? (cudaStream_t)s->o.stream : s->stream;
+  if (s->graph && c->done && graph_key(s, d, l, c) == s->graph_key) {
+    ADS_CUDA(cudaStreamWaitEvent(st, c->done, 0));
+    c->pending = true;
+    c->count = 0;
+    ADS_CUDA(cudaGraphLaunch(s->graph, st));
+    s->last_launches = s->graph_launches;
+    ADS_CUDA(cudaEventRecord(c->done, st));
+    return ADS_OK;
+  }
+  ADS_TRY(enqueue_search(s, d, l, c, false));
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  const int64_t launches = s->last_launches;
+  cudaGraph_t g = nullptr;
+  ADS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  const int rc = enqueue_search(s, d, l, c, true);
+  const cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (rc != ADS_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate", __FILE__, __LINE__);
+  s->graph = ex;
+  s->graph_key = graph_key(s, d, l, c);
+  s->graph_launches = launches;
+  s->last_launches = launches;
   return ADS_OK;
 }
 
@@ -952,6 +1097,7 @@ int ads_selection_destroy(AdsSelection* s) {
     if (!s) return ADS_OK;
     DeviceGuard dg(s->device);
     cudaStreamSynchronize(s->stream);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     for (auto& set : s->stage_pool)
@@ -1025,6 +1171,11 @@ int ads_candidates_create(const AdsSelection* s, AdsCandidates** out) {
     *out = c.release();
     return ADS_OK;
   });
+}
+
+int ads_selection_autotune(AdsSelection* s, const AdsDia* d, const AdsLib* l, int32_t repeats,
+                           int32_t* warps_per_block, int32_t* cycles_per_lane, float* best_ms) {
+  return guarded([&] { return autotune(s, d, l, repeats, warps_per_block, cycles_per_lane, best_ms); });
 }
 
 int ads_select_async(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidates* c) {

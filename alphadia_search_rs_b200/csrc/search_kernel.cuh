@@ -145,21 +145,18 @@ static __device__ __noinline__ void add_chunk_grouped(bool inc, int cell, int ad
 
 // Adds one chunk of 32 CSR-consecutive entries to the XIC row in lane order (the
 // reference's `dense_xic[c] += intensity`, src/quadrupole_observation/mod.rs:96-105).
-// A tag per cycle detects whether two accepted lanes hit the same cycle; only then
-// are the lanes grouped and summed by their lowest lane one rounded add at a time.
-// Tags only grow (seq), so stale tags from earlier chunks never hide a collision.
+// Every accepted lane writes its lane number into its cycle's tag; a lane that
+// reads back another number shares the cycle, and only then are the lanes grouped
+// and summed by their lowest lane one rounded add at a time.
 __device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v, int lane,
                                           float* row, uint32_t* bm, uint32_t* tags, float* scr,
-                                          uint32_t& seq, unsigned long long& n_acc) {
+                                          unsigned long long& n_acc) {
   const unsigned act = __ballot_sync(kFull, inc);
   if (act == 0) return;
   n_acc += __popc(act);
-  const uint32_t mytag = (seq << 5) | (uint32_t)lane;
-  ++seq;
-  uint32_t old = 0;
-  if (inc) old = atomicMax(tags + cell, mytag);
+  if (inc) tags[cell] = (uint32_t)lane;
   __syncwarp();
-  const bool dup = inc && (tags[cell] != mytag || (old >> 5) == (mytag >> 5));
+  const bool dup = inc && tags[cell] != (uint32_t)lane;
   const int bit = cell + kBitOff;
   if (!__any_sync(kFull, dup)) {
     if (inc) {
@@ -227,7 +224,7 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
                                             uint32_t b0, uint32_t b1, int64_t rs, int64_t re,
                                             int cs, int ce, int lane, float* row, int off,
                                             uint32_t* bm, uint32_t* tags, float* scr,
-                                            uint32_t& seq, Counters& k) {
+                                            Counters& k) {
   const int64_t n = re - rs;
   if (n <= 0) return;
   const uint16_t* cy = a.cyc + wbase;
@@ -259,8 +256,7 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
           inc = last;
         }
         const int cell = cu - cs;
-        add_chunk(inc, cell, inc ? xaddr<S>(cell + off) : 0, v[u], lane, row, bm, tags, scr, seq,
-                  k.acc);
+        add_chunk(inc, cell, inc ? xaddr<S>(cell + off) : 0, v[u], lane, row, bm, tags, scr, k.acc);
       }
     }
   } else {
@@ -301,7 +297,7 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
         const int c = vt ? (int)__ldg(cy + q) : 0;
         const float v = vt ? ld_intensity<FAST>(a, wbase + q) : 0.0f;
         const int cell = c - cs;
-        add_chunk(vt, cell, vt ? xaddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, seq, k.acc);
+        add_chunk(vt, cell, vt ? xaddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, k.acc);
       }
     }
   }
@@ -420,10 +416,8 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
 
   for (int i = threadIdx.x; i < kLnTableSize; i += blockDim.x) lnt[i] = a.ln_tab[i];
   for (int i = threadIdx.x; i <= a.h; i += blockDim.x) kw_s[i] = a.kw[i];
-  for (int i = lane; i < a.ncell; i += 32) tags[i] = 0u;
   __syncthreads();
   Counters k;
-  uint32_t seq = 1;
 
   const unsigned long long n_work = a.list ? (unsigned long long)*a.list_len
                                             : (unsigned long long)a.n_prec;
@@ -452,11 +446,6 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
     const int passes = (C + 32 * S - 1) / (32 * S);
     k.frag += F;
     for (int i = lane; i <= C + C / S; i += 32) score[i] = 0.0f;  // cycles [0, C) with pads
-    if (seq >= (1u << 26)) {  // keep tag << 5 inside 32 bits
-      __syncwarp();
-      for (int i = lane; i < a.ncell; i += 32) tags[i] = 0u;
-      seq = 1;
-    }
 
     // CSR ranges of up to 32 (fragment, window) pairs, fetched together: lane q
     // holds pair pb + q
@@ -508,7 +497,7 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
         k.pairs += 1;
         k.bins1 += qb1 - qb0 + 1;
         gather_pair<S, FAST>(a, qw, qbase, qb0, qb1, qrs, qre, cs, ce, lane, row, P.off, bm, tags,
-                             scr, seq, k);
+                             scr, k);
       }
       __syncwarp();
       const float wf = __ldg(a.fw + p * a.kf + f);
@@ -549,18 +538,18 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
             }
             cvb[m] = s;
           }
-          // score terms of the valid outputs [m0, m1), two at a time; a zero output
-          // adds ln(1) * w = +0, which leaves the score as it is
+          // score terms, two at a time with the same trip count in every lane; a zero
+          // output, and every output outside the valid range [m0, m1), adds
+          // ln(1) * w = +0, which leaves the score as it is (slot S is a pad word)
           const int m0 = max(H - j0, 0), m1 = min(C - H - j0, S);
-          int m = m0;
 #pragma unroll 1
-          for (; m + 1 < m1; m += 2) {
-            const float c0 = cvb[m], c1 = cvb[m + 1];
+          for (int m = 0; m < S; m += 2) {
+            const float c0 = (m >= m0 && m < m1) ? cvb[m] : 0.0f;
+            const float c1 = (m + 1 >= m0 && m + 1 < m1) ? cvb[m + 1] : 0.0f;
             const float s0 = sb[m], s1 = sb[m + 1];
             sb[m] = score_term<FAST>(s0, c0, wf, lnt);
             sb[m + 1] = score_term<FAST>(s1, c1, wf, lnt);
           }
-          if (m < m1) sb[m] = score_term<FAST>(sb[m], cvb[m], wf, lnt);
         } else {
           for (int m = 0; m < S; ++m) {
             const int j = j0 + m;

@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--warps-per-block", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--cycles-per-lane", type=int, default=0)
+    ap.add_argument("--graph", action="store_true",
+                    help="replay a captured CUDA graph per search (stage times then come "
+                         "from a second, directly enqueued pass)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick warps per block and cycles per lane with the engine's autotuner")
     ap.add_argument("--precision", choices=["fp32", "bf16"], default=None,
                     help="override the workload's precision (cfg3/cfg4: bf16 storage)")
     return ap.parse_args()
@@ -385,16 +390,22 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.empty_cache()
 
     sel = ads.PeakGroupSelection(params, verbose=False, device=local_rank, time_stages=True,
-                                 precision=precision,
+                                 precision=precision, use_graph=args.graph,
                                  warps_per_block=args.warps_per_block,
                                  cycles_per_lane=args.cycles_per_lane,
                                  blocks_per_sm=args.blocks_per_sm)
+    tuned = sel.autotune(dia, slib) if args.autotune else None
+    sel_opts = ((tuned["warps_per_block"], tuned["cycles_per_lane"]) if tuned
+                else (args.warps_per_block, args.cycles_per_lane))
     cand = sel.new_candidates()
     stream = torch.cuda.ExternalStream(sel.stream, device=device)
     for _ in range(args.warmup):
         sel.search_into(dia, slib, cand)
     cand.size()
-    sel.stage_times()  # discard warm-up stage timings
+    try:
+        sel.stage_times()  # discard warm-up stage timings
+    except ValueError:  # graph replays record none
+        pass
     launches_per_step = sel.last_launches
 
     dist = world > 1
@@ -416,7 +427,25 @@ def run_ours(args, rank, world, local_rank):
     ms = ev0.elapsed_time(ev1)
     if cand.size() != n_cand:
         raise RuntimeError("candidate count changed between searches")
-    st = sel.stage_times()
+    if not args.graph:
+        st = sel.stage_times()
+    else:
+        # graph replays record no stage events: time the stages on a second pass of
+        # the same searches enqueued directly
+        sel_st = ads.PeakGroupSelection(params, verbose=False, device=local_rank, time_stages=True,
+                                        precision=precision, warps_per_block=sel_opts[0],
+                                        cycles_per_lane=sel_opts[1],
+                                        blocks_per_sm=args.blocks_per_sm)
+        cand_st = sel_st.new_candidates()
+        for _ in range(args.warmup):
+            sel_st.search_into(dia, slib, cand_st)
+        cand_st.size()
+        sel_st.stage_times()
+        for _ in range(args.steps):
+            sel_st.search_into(dia, slib, cand_st)
+        cand_st.size()
+        st = sel_st.stage_times()
+        del cand_st, sel_st
     ms_t = torch.tensor([ms], device=device, dtype=torch.float64)
     if dist:
         td.all_reduce(ms_t, op=td.ReduceOp.MAX)
@@ -519,7 +548,10 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (resident run ~%.1f GB), no flush" %
                          (dia.memory_footprint_bytes() / 1e9),
                    "peaks": n_peaks_total, "candidates_per_step": int(n_cand),
-                   "precursors_per_gpu": int(P), "parallelism": f"replicated run, {world} library shard(s)"},
+                   "precursors_per_gpu": int(P), "parallelism": f"replicated run, {world} library shard(s)",
+                   "launch": {"cuda_graph": bool(args.graph), "autotuned": tuned,
+                              "warps_per_block": sel_opts[0] or "default",
+                              "cycles_per_lane": sel_opts[1] or "length classes"}},
         "e2e": {"value": e2e_value, "unit": "precursors/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
                 "path": "SpecLibFlat.from_arrays(pinned host arrays) + PeakGroupSelection.search + "

@@ -249,6 +249,17 @@ int ads_selection_last_stats(AdsSelection* sel, int64_t* out, int64_t cap);
  * [0] prep kernel, [1] search kernel, [2] compaction kernels (sums), [3] number of
  * searches.  Waits for the last recorded search. */
 int ads_selection_stage_times(AdsSelection* sel, float* ms, int64_t cap);
+/* Autotuner (an engine addition; the reference has no launch shapes to tune).
+ * Times the search of `dia` x `lib` (`repeats` timed searches per shape, after
+ * one warm-up) for warps per block 2, 4, 8 (precursors in flight per CTA) and cycles
+ * per lane 0 (length classes), 4, 8, 10, 13, 16 (cycles per tile = 32 x that),
+ * keeps the fastest in the selection's options and caches it per workload shape
+ * (device, precision, kernel half width, longest RT window, precursors, fragments)
+ * for the process.  Writes the choice and its mean ms where the pointers are not
+ * NULL.  Blocks until done. */
+int ads_selection_autotune(AdsSelection* sel, const AdsDia* dia, const AdsLib* lib,
+                           int32_t repeats, int32_t* warps_per_block, int32_t* cycles_per_lane,
+                           float* best_ms);
 
 /* ------------------------------------------------------- CandidateCollection
  * CandidateCollection.len / to_arrays (src/candidate/entry.rs:61-173). */

@@ -63,6 +63,44 @@ def test_search_bit_exact_every_lane_width(workload, cycles_per_lane):
     assert_candidates_equal(got, ref, exact_scores=True, where=f"{cfg.name}/S{cycles_per_lane}")
 
 
+def test_graph_replay_matches_direct(workload):
+    """use_graph: the first search runs directly and is captured; the next ones
+    replay the graph (into the same collection) and give the same candidates."""
+    cfg, run, la, _ = workload
+    ref, dia, lib, _ = product_search(run, la, cfg.params_dict())
+    from alphadia_search_rs_b200 import PeakGroupSelection
+
+    from _util import COLS, params_from
+
+    sel = PeakGroupSelection(params_from(cfg.params_dict()), verbose=False, use_graph=True)
+    cand = sel.new_candidates()
+    for call in range(3):
+        sel.search_into(dia, lib, cand)
+        n = cand.size()
+        got = {c: np.zeros(n, np.float32 if c == "score" else np.uint64) for c in COLS}
+        cand.copy_out(got)
+        assert_candidates_equal(got, ref, exact_scores=True, where=f"{cfg.name}/graph call {call}")
+
+
+def test_autotune_keeps_results(workload):
+    """The autotuner only changes launch shapes: the tuned search gives the same
+    candidates, and a second call is served from the cache."""
+    cfg, run, la, _ = workload
+    ref, dia, lib, _ = product_search(run, la, cfg.params_dict())
+    from alphadia_search_rs_b200 import PeakGroupSelection
+
+    from _util import COLS, params_from
+
+    sel = PeakGroupSelection(params_from(cfg.params_dict()), verbose=False)
+    choice = sel.autotune(dia, lib, repeats=1)
+    assert choice["warps_per_block"] in (2, 4, 8)
+    assert choice["cycles_per_lane"] in (0, 4, 8, 10, 13, 16)
+    assert choice["ms"] > 0
+    assert sel.autotune(dia, lib) == choice
+    got = dict(zip(COLS, sel.search(dia, lib).to_arrays()))
+    assert_candidates_equal(got, ref, exact_scores=True, where=f"{cfg.name}/tuned {choice}")
+
+
 def test_search_vs_reference_numerics(workload):
     cfg, run, la, (od, ol, tol) = workload
     got, *_ = product_search(run, la, cfg.params_dict())
