@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a) {
 // Cycles per lane the search kernel is compiled for, and its instances: fully
 // unrolled stencils for the half widths of kernel_size 20, 21-22 and 31-32, any
 // other half width through the generic path.
-constexpr int kLaneCycles[] = {4, 8, 10, 13, 16};
+constexpr int kLaneCycles[] = {4, 8, 10, 12, 16};
 constexpr int kMaxClasses = 6;
 
 // Length classes of one search: class b covers C <= bound[b] with S[b] cycles per
@@ -345,7 +345,7 @@ void (*pick_for_h(int S))(SearchArgs) {
     case 4: return search_kernel<H, 4, FAST>;
     case 8: return search_kernel<H, 8, FAST>;
     case 10: return search_kernel<H, 10, FAST>;
-    case 13: return search_kernel<H, 13, FAST>;
+    case 12: return search_kernel<H, 12, FAST>;
     default: return search_kernel<H, 16, FAST>;
   }
 }
@@ -363,6 +363,19 @@ void (*pick_for_precision(int h, int S))(SearchArgs) {
 // fast: BF16 intensity storage with the fast f32 arithmetic (ADS_PRECISION_BF16)
 void (*pick_search_kernel(int h, int S, bool fast))(SearchArgs) {
   return fast ? pick_for_precision<true>(h, S) : pick_for_precision<false>(h, S);
+}
+
+// Kernel taps w[0..h] of a launch, also each twice as one packed f32x2 operand,
+// and the packed zeros of the exact stencil.
+void set_taps(SearchArgs* sa, const float* kernel, int h) {
+  for (int k = 0; k <= h; ++k) {
+    sa->kw[k] = kernel[k];
+    uint32_t b;
+    std::memcpy(&b, &kernel[k], 4);
+    sa->kw2[k] = ((unsigned long long)b << 32) | b;
+  }
+  sa->zero2 = 0ull;
+  sa->nzero2 = 0x8000000080000000ull;
 }
 
 // ------------------------------------------------------------ compaction
@@ -659,7 +672,7 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
   const int S_fixed = s->o.cycles_per_lane;
   if (S_fixed != 0 &&
       std::find(std::begin(kLaneCycles), std::end(kLaneCycles), S_fixed) == std::end(kLaneCycles))
-    return fail(ADS_ERR_INVALID_ARGUMENT, "cycles_per_lane must be 0 or one of 4, 8, 10, 13, 16");
+    return fail(ADS_ERR_INVALID_ARGUMENT, "cycles_per_lane must be 0 or one of 4, 8, 10, 12, 16");
   LenClasses cls;
   const int n_cls = plan_classes(c_max, S_fixed, &cls);
   const int S_last = cls.S[n_cls - 1];
@@ -785,7 +798,7 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
   sa.inten = d->intens.p;
   sa.inten_bf16 = d->intens_bf16.p;
   sa.ln_tab = ln_tab;
-  for (int k = 0; k <= s->h; ++k) sa.kw[k] = s->kernel[k];
+  set_taps(&sa, s->kernel.data(), s->h);
   sa.h = s->h;
   sa.k_out = k_out;
   sa.gather_mode = s->o.gather_mode;
@@ -912,7 +925,7 @@ int autotune(AdsSelection* s, const AdsDia* d, const AdsLib* l, int32_t repeats,
     scratch.device = s->device;
     int rc = ADS_OK;
     for (int nw : {2, 4, 8}) {
-      for (int S : {0, 4, 8, 10, 13, 16}) {
+      for (int S : {0, 4, 8, 10, 12, 16}) {
         if (S != 0 && (int64_t)32 * S * 8 < key.c_max) continue;  // more than 8 passes
         s->o.warps_per_block = nw;
         s->o.cycles_per_lane = S;
@@ -1462,7 +1475,7 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   sa.cyc = d->cycles.p;
   sa.inten = d->intens.p;
   sa.ln_tab = reinterpret_cast<const double2*>(base);
-  for (int k = 0; k <= h; ++k) sa.kw[k] = kernel[k];
+  set_taps(&sa, kernel.data(), h);
   sa.h = h;
   sa.k_out = k_out;
   sa.c_max = (int)c_max;

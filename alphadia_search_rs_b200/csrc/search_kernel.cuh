@@ -39,6 +39,9 @@ struct SearchArgs {
   const uint16_t* inten_bf16;  // bfloat16 copy of `inten` (BF16-storage searches)
   const double2* ln_tab;
   float kw[kMaxHalf + 1];  // kernel taps w[0..h]; w[h] is the centre
+  unsigned long long kw2[kMaxHalf + 1];  // the same taps, each twice (packed f32x2 operands)
+  unsigned long long zero2;   // +0.0f twice
+  unsigned long long nzero2;  // -0.0f twice
   int h;
   int k_out;   // candidates kept per precursor
   int c_max;   // largest cycle range of the precursors this launch searches
@@ -59,13 +62,26 @@ constexpr int kMaxCycles = 2048;    // longest RT window (cycles) a precursor ma
 
 __host__ __device__ inline int maxima_cap(int ncell) { return ncell / 4 + 8; }
 
-// Shared-memory address of stored index i (cycle + off) in a row or score array
-// whose lanes own S consecutive cycles: one pad word after every S cells, so that
-// the 32 lanes of a warp, reading at the same offset within their segments, hit
-// 32 different banks.
+// Shared-memory address of stored index i (cycle + off) in a score array whose
+// lanes own S consecutive cycles: one pad word after every S cells, so that the 32
+// lanes of a warp, reading at the same offset within their segments, hit 32
+// different banks.
 template <int S>
 __device__ __forceinline__ int xaddr(int i) {
   return i + i / S;
+}
+
+// The XIC row is read as 8-byte pairs of cells (u, u + 1), u even within a lane's
+// segment, so its segments of S cells (S even) sit at an even stride of
+// row_stride(S) words whose half is odd: the 16 lanes of each half-warp then hit 16
+// different bank pairs.
+__host__ __device__ constexpr int row_stride(int S) {
+  return ((S + 2) / 2) % 2 == 1 ? S + 2 : S + 4;
+}
+
+template <int S>
+__device__ __forceinline__ int raddr(int i) {
+  return i + (i / S) * (row_stride(S) - S);
 }
 
 // Floor division, for offsets known at compile time.
@@ -76,7 +92,7 @@ __host__ __device__ constexpr int floordiv(int a, int b) {
 // Per-warp shared-memory plan, in 4-byte words.  The block's ln table (double2 x
 // 256 = 1024 words) and kernel taps (32 words) come first.
 struct WarpPlan {
-  int row, tags, bm, scr, score, cvb, mval, midx, total;
+  int row, tags, bm, scr, score, lst, mval, midx, total;
   int off;        // stored index of cycle c is c + off (off >= h, a multiple of S)
   int row_words;  // words of the row, a multiple of 4
   int bw;         // bitmap words
@@ -88,7 +104,7 @@ __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
   WarpPlan w;
   w.off = (h + S - 1) / S * S;
   const int span = ncell + h + w.off + S;  // stored indices [0, span) cover every read
-  w.row_words = (span + span / S + 1 + 3) & ~3;
+  w.row_words = (span + (span / S + 1) * (row_stride(S) - S) + 3) & ~3;
   int o = 0;
   w.row = o;
   o += w.row_words;
@@ -101,8 +117,9 @@ __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
   o += 32;
   w.score = o + 4;  // 4 words of margin below: the maxima scan reads 2 cycles early
   o += ncell + ncell / S + 12;
-  w.cvb = o;  // one pass of convolved values, lane l at l * (S + 1)
-  o += 32 * (S + 1);
+  o = (o + 1) & ~1;
+  w.lst = o;  // one pass of non-zero convolved values: (value, score address) pairs
+  o += 2 * 32 * S;
   w.mx = maxima_cap(ncell);
   w.mval = o;
   o += w.mx;
@@ -256,7 +273,7 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
           inc = last;
         }
         const int cell = cu - cs;
-        add_chunk(inc, cell, inc ? xaddr<S>(cell + off) : 0, v[u], lane, row, bm, tags, scr, k.acc);
+        add_chunk(inc, cell, inc ? raddr<S>(cell + off) : 0, v[u], lane, row, bm, tags, scr, k.acc);
       }
     }
   } else {
@@ -297,7 +314,7 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
         const int c = vt ? (int)__ldg(cy + q) : 0;
         const float v = vt ? ld_intensity<FAST>(a, wbase + q) : 0.0f;
         const int cell = c - cs;
-        add_chunk(vt, cell, vt ? xaddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, k.acc);
+        add_chunk(vt, cell, vt ? raddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, k.acc);
       }
     }
   }
@@ -317,6 +334,41 @@ __device__ __forceinline__ bool bits_any(const uint32_t* bm, int lo, int n) {
   return acc != 0u;
 }
 
+// Packed f32x2 arithmetic (sm_100a): one instruction performs two independent f32
+// operations, each rounded to nearest exactly like __fadd_rn / __fmul_rn /
+// __fmaf_rn, so a packed result is bit-identical to the two scalar ones.
+//
+// ptxas contracts a packed multiply followed by a packed add into one fused
+// multiply-add even with explicit .rn rounding and --fmad=false (measured on
+// sm_100a: about half of 12-term chains differed).  The exact path therefore forms
+// each rounded product as fma(a, b, -0), with the -0 a kernel argument that ptxas
+// cannot see: fma(a, b, -0) = round(a * b) bit for bit, and an fma followed by an
+// add is not contractible.  The +0 of the reference's `0 + x * w` is a kernel
+// argument for the same reason.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pk2(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+
+__device__ __forceinline__ void unpk2(f32x2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 // One output of convolution_scalar (src/convolution/scalar.rs:30-50) read from the
 // row in shared memory: x[j]*w[h] first, then (x[j-d] + x[j+d]) * w[h-d] for
 // d = h..1.  Any half width; used off the main path.  FAST (BF16 storage) fuses
@@ -324,9 +376,9 @@ __device__ __forceinline__ bool bits_any(const uint32_t* bm, int lo, int n) {
 template <int S, bool FAST>
 __device__ __forceinline__ float conv_at(const float* row, int off, const float* kw_s, int h,
                                          int j) {
-  float s = __fadd_rn(0.0f, __fmul_rn(row[xaddr<S>(j + off)], kw_s[h]));
+  float s = __fadd_rn(0.0f, __fmul_rn(row[raddr<S>(j + off)], kw_s[h]));
   for (int t = 0; t < h; ++t) {
-    const float lr = __fadd_rn(row[xaddr<S>(j - h + t + off)], row[xaddr<S>(j + h - t + off)]);
+    const float lr = __fadd_rn(row[raddr<S>(j - h + t + off)], row[raddr<S>(j + h - t + off)]);
     s = FAST ? __fmaf_rn(lr, kw_s[t], s) : __fadd_rn(s, __fmul_rn(lr, kw_s[t]));
   }
   return s;
@@ -410,7 +462,6 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
   uint32_t* bm = reinterpret_cast<uint32_t*>(wb + P.bm);
   float* scr = wb + P.scr;
   float* score = wb + P.score;
-  float* cvb = wb + P.cvb + lane * (S + 1);
   float* mval = wb + P.mval;
   int* midx = reinterpret_cast<int*>(wb + P.midx);
 
@@ -445,6 +496,8 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
     const int npairs = F * nwin;
     const int passes = (C + 32 * S - 1) / (32 * S);
     k.frag += F;
+    // fragment weights, lane f holding fragment f's (fetched once per precursor)
+    const float wf_lane = lane < F ? __ldg(a.fw + p * a.kf + lane) : 0.0f;
     for (int i = lane; i <= C + C / S; i += 32) score[i] = 0.0f;  // cycles [0, C) with pads
 
     // CSR ranges of up to 32 (fragment, window) pairs, fetched together: lane q
@@ -500,7 +553,8 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
                              scr, k);
       }
       __syncwarp();
-      const float wf = __ldg(a.fw + p * a.kf + f);
+      float wf = __shfl_sync(kFull, wf_lane, f & 31);
+      if (f >= 32) wf = __ldg(a.fw + p * a.kf + f);
       if (!isfinite(wf)) {
         // ln(conv + 1) * inf is NaN even where conv is zero: every column takes
         // its term, as in the reference
@@ -512,52 +566,88 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
         continue;
       }
       if (k.acc == acc0) continue;  // empty row: every term is +0
-      // ---- 2./3. convolution of this lane's cycles and their score terms; a zero
-      // output adds ln(1) * w = +0 and is skipped
+      // ---- 2./3. convolution of this lane's cycles, then the score terms of its
+      // non-zero outputs.  A zero output adds ln(1) * w = +0, which leaves a score as
+      // it is, so only non-zero outputs of the valid range [h, C - h) are listed
+      // (warp-compacted, in lane order) and take a logarithm.
+      float2* lst = reinterpret_cast<float2*>(wb + P.lst);
       for (int ps = 0; ps < passes; ++ps) {
         const int j0 = ps * 32 * S + lane * S;
-        if (j0 + S <= h || j0 >= C - h) continue;  // no valid output [h, C - h) here
-        if (!bits_any(bm, j0 - h + kBitOff, S + 2 * h)) continue;
+        const bool act = j0 + S > h && j0 < C - h && bits_any(bm, j0 - h + kBitOff, S + 2 * h);
+        if (!__any_sync(kFull, act)) continue;
+        uint32_t mk = 0;
+        float cv[S];
         if (H > 0) {
-          // cycle j0 + u sits at rb[u + floor(u / S)]; its score at sb[u] (0 <= u < S)
-          const float* rb = row + (ps * 32 + lane + P.off / S) * (S + 1);
-          float* sb = score + (ps * 32 + lane) * (S + 1);
-          float x[S + 2 * H];
+          if (act) {
+            // cells u in [UB, UE) of this lane's segment as 8-byte pairs (u even);
+            // every output is formed in the reference's order: 0 + x[j]*w[h], then
+            // + (x[j-d] + x[j+d]) * w[h-d] for d = h..1, two outputs (m, m + 1) per
+            // packed instruction.  For odd d the pair sums straddle the register
+            // pairs and are formed by two scalar adds.
+            constexpr int UB = -((H + 1) & ~1);
+            constexpr int UE = (S + H + 1) & ~1;
+            constexpr int NX = UE - UB;
+            const float* rb = row + (ps * 32 + lane + P.off / S) * row_stride(S);
+            float xv[NX];
 #pragma unroll
-          for (int t = 0; t < S + 2 * H; ++t) x[t] = rb[(t - H) + floordiv(t - H, S)];
-          // each output in the reference's order: 0 + x[j]*w[h], then
-          // + (x[j-d] + x[j+d]) * w[h-d] for d = h..1; parked in this lane's cvb
-          // slots so that the log below exists once in the code
-#pragma unroll
-          for (int m = 0; m < S; ++m) {
-            float s = __fadd_rn(0.0f, __fmul_rn(x[m + H], a.kw[H]));
-#pragma unroll
-            for (int t = 0; t < H; ++t) {
-              const float lr = __fadd_rn(x[m + t], x[m + 2 * H - t]);
-              s = FAST ? __fmaf_rn(lr, a.kw[t], s) : __fadd_rn(s, __fmul_rn(lr, a.kw[t]));
+            for (int q = 0; q < NX; q += 2) {
+              const int u = UB + q;
+              const float2 v =
+                  *reinterpret_cast<const float2*>(rb + u + floordiv(u, S) * (row_stride(S) - S));
+              xv[q] = v.x;
+              xv[q + 1] = v.y;
             }
-            cvb[m] = s;
+#pragma unroll
+            for (int m = 0; m < S; m += 2) {
+              f32x2 acc = add2(a.zero2, fma2(pk2(xv[m - UB], xv[m + 1 - UB]), a.kw2[H], a.nzero2));
+#pragma unroll
+              for (int t = 0; t < H; ++t) {
+                const int d = H - t;
+                f32x2 lr;
+                if (d % 2 == 0)
+                  lr = add2(pk2(xv[m - d - UB], xv[m - d + 1 - UB]),
+                            pk2(xv[m + d - UB], xv[m + d + 1 - UB]));
+                else
+                  lr = pk2(__fadd_rn(xv[m - d - UB], xv[m + d - UB]),
+                           __fadd_rn(xv[m + 1 - d - UB], xv[m + 1 + d - UB]));
+                acc = FAST ? fma2(lr, a.kw2[t], acc) : add2(acc, fma2(lr, a.kw2[t], a.nzero2));
+              }
+              unpk2(acc, cv[m], cv[m + 1]);
+            }
           }
-          // score terms, two at a time with the same trip count in every lane; a zero
-          // output, and every output outside the valid range [m0, m1), adds
-          // ln(1) * w = +0, which leaves the score as it is (slot S is a pad word)
-          const int m0 = max(H - j0, 0), m1 = min(C - H - j0, S);
-#pragma unroll 1
-          for (int m = 0; m < S; m += 2) {
-            const float c0 = (m >= m0 && m < m1) ? cvb[m] : 0.0f;
-            const float c1 = (m + 1 >= m0 && m + 1 < m1) ? cvb[m + 1] : 0.0f;
-            const float s0 = sb[m], s1 = sb[m + 1];
-            sb[m] = score_term<FAST>(s0, c0, wf, lnt);
-            sb[m + 1] = score_term<FAST>(s1, c1, wf, lnt);
-          }
-        } else {
+        } else if (act) {
+#pragma unroll
           for (int m = 0; m < S; ++m) {
             const int j = j0 + m;
-            if (j < h || j >= C - h) continue;
-            const float s = conv_at<S, FAST>(row, P.off, kw_s, h, j);
-            if (s != 0.0f) score_add<FAST>(score, xaddr<S>(j), s, wf, lnt);
+            cv[m] = (j >= h && j < C - h) ? conv_at<S, FAST>(row, P.off, kw_s, h, j) : 0.0f;
           }
         }
+        if (act) {
+          const int m0 = max(h - j0, 0), m1 = min(C - h - j0, S);
+#pragma unroll
+          for (int m = 0; m < S; ++m)
+            mk |= (uint32_t)(m >= m0 && m < m1 && cv[m] != 0.0f) << m;
+        }
+        const int cnt = __popc(mk);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += t;
+        }
+        const int total = __shfl_sync(kFull, incl, 31);
+        int pos = incl - cnt;
+        const int sbase = (ps * 32 + lane) * (S + 1);  // score address of cycle j0
+#pragma unroll
+        for (int m = 0; m < S; ++m)
+          if ((mk >> m) & 1u) lst[pos++] = make_float2(cv[m], __int_as_float(sbase + m));
+        __syncwarp();
+        for (int i = lane; i < total; i += 32) {
+          const float2 e = lst[i];
+          const int at = __float_as_int(e.y);
+          score[at] = score_term<FAST>(score[at], e.x, wf, lnt);
+        }
+        __syncwarp();
       }
       __syncwarp();
     }

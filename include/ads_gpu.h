@@ -167,7 +167,7 @@ typedef struct {
   int32_t gather_mode;     /* 0 = automatic, 1 = always scan bin ranges, 2 = always
                               binary-search each bin (both are exact; for testing) */
   int32_t time_stages;     /* 1: record CUDA events around each stage of a search */
-  int32_t cycles_per_lane; /* 0 = chosen from the longest RT window; else 4, 8, 10, 13
+  int32_t cycles_per_lane; /* 0 = chosen from the longest RT window; else 4, 8, 10, 12
                               or 16 consecutive cycles per lane of the search kernel */
   int64_t stream;          /* cudaStream_t to run on, 0 = the handle's own stream */
 } AdsEngineOptions;
@@ -252,7 +252,7 @@ int ads_selection_stage_times(AdsSelection* sel, float* ms, int64_t cap);
 /* Autotuner (an engine addition; the reference has no launch shapes to tune).
  * Times the search of `dia` x `lib` (`repeats` timed searches per shape, after
  * one warm-up) for warps per block 2, 4, 8 (precursors in flight per CTA) and cycles
- * per lane 0 (length classes), 4, 8, 10, 13, 16 (cycles per tile = 32 x that),
+ * per lane 0 (length classes), 4, 8, 10, 12, 16 (cycles per tile = 32 x that),
  * keeps the fastest in the selection's options and caches it per workload shape
  * (device, precision, kernel half width, longest RT window, precursors, fragments)
  * for the process.  Writes the choice and its mean ms where the pointers are not
