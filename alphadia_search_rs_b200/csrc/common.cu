@@ -26,6 +26,64 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
   return e == cudaErrorMemoryAllocation ? ADS_ERR_OUT_OF_MEMORY : ADS_ERR_CUDA;
 }
 
+// ------------------------------------------------------------ device memory
+
+namespace {
+struct DevicePool {
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t stream = nullptr;
+};
+std::mutex g_pool_mu;
+std::map<int, DevicePool> g_pools;
+
+int device_pool(int device, DevicePool* out) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pools.find(device);
+  if (it != g_pools.end()) {
+    *out = it->second;
+    return ADS_OK;
+  }
+  DeviceGuard dg(device);
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  DevicePool dp;
+  ADS_CUDA(cudaMemPoolCreate(&dp.pool, &props));
+  uint64_t keep = kPoolKeepBytes;
+  ADS_CUDA(cudaMemPoolSetAttribute(dp.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  ADS_CUDA(cudaStreamCreateWithFlags(&dp.stream, cudaStreamNonBlocking));
+  g_pools[device] = dp;
+  *out = dp;
+  return ADS_OK;
+}
+}  // namespace
+
+int pool_alloc(int device, size_t bytes, void** out) {
+  *out = nullptr;
+  DevicePool dp;
+  ADS_TRY(device_pool(device, &dp));
+  cudaError_t e = cudaMallocFromPoolAsync(out, bytes, dp.pool, dp.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(dp.stream);  // usable on every stream
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return cuda_fail(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
+  }
+  return ADS_OK;
+}
+
+void pool_free(int device, void* p) {
+  DevicePool dp;
+  if (device_pool(device, &dp) != ADS_OK) return;
+  DeviceGuard dg(device);
+  cudaDeviceSynchronize();  // nothing in flight may still read or write p
+  cudaFreeAsync(p, dp.stream);
+  cudaStreamSynchronize(dp.stream);
+  cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- m/z grid
 
 // MZIndex::new / ppm_index (src/mz_index/mod.rs:8-25, 41-45): f32 geometric

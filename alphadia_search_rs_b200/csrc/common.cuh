@@ -64,15 +64,27 @@ struct DeviceGuard {
   }
 };
 
-// Owning device buffer (move-only).
+// ------------------------------------------------------------ device memory
+// Every device buffer of the engine comes from one memory pool per device that
+// keeps up to kPoolKeepBytes of freed memory for reuse, so that building a
+// library or a candidate collection per call does not map and unmap device pages
+// each time.  Allocation and release are ordered on a private stream of the pool;
+// a release first waits for the device to go idle (the guarantee cudaFree gives),
+// so no kernel still in flight can see its memory handed out again.
+constexpr uint64_t kPoolKeepBytes = uint64_t(4) << 30;
+int pool_alloc(int device, size_t bytes, void** out);
+void pool_free(int device, void* p);
+
+// Owning device buffer (move-only) on the current device's pool.
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  int dev = -1;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), dev(o.dev) {
     o.p = nullptr;
     o.n = 0;
   }
@@ -81,6 +93,7 @@ struct DevBuf {
       release();
       p = o.p;
       n = o.n;
+      dev = o.dev;
       o.p = nullptr;
       o.n = 0;
     }
@@ -88,22 +101,22 @@ struct DevBuf {
   }
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) pool_free(dev, p);
     p = nullptr;
     n = 0;
   }
-  // Allocates exactly `count` elements (frees the previous buffer).
+  // Allocates exactly `count` elements on the current device (frees the previous
+  // buffer).
   int alloc(size_t count) {
     release();
     if (count == 0) return ADS_OK;
+    int d = 0;
+    ADS_CUDA(cudaGetDevice(&d));
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
-    }
+    ADS_TRY(pool_alloc(d, count * sizeof(T), &q));
     p = static_cast<T*>(q);
     n = count;
+    dev = d;
     return ADS_OK;
   }
   // Grows to at least `count` elements, keeping nothing.
