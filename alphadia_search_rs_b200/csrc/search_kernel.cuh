@@ -59,6 +59,8 @@ struct SearchArgs {
 constexpr int kPrefetchChunks = 4;  // 4 x 32 CSR entries read per round trip
 constexpr int kBitOff = 32;         // bitmap bit of cycle c is c + kBitOff (room for -h)
 constexpr int kMaxCycles = 2048;    // longest RT window (cycles) a precursor may span
+constexpr int kTouchCap = 256;      // cells a row records for clearing; beyond it the row is
+                                    // zeroed whole
 
 __host__ __device__ inline int maxima_cap(int ncell) { return ncell / 4 + 8; }
 
@@ -92,7 +94,7 @@ __host__ __device__ constexpr int floordiv(int a, int b) {
 // Per-warp shared-memory plan, in 4-byte words.  The block's ln table (double2 x
 // 256 = 1024 words) and kernel taps (32 words) come first.
 struct WarpPlan {
-  int row, tags, bm, scr, score, lst, mval, midx, total;
+  int row, tags, bm, scr, score, lst, mval, midx, touched, total;
   int off;        // stored index of cycle c is c + off (off >= h, a multiple of S)
   int row_words;  // words of the row, a multiple of 4
   int bw;         // bitmap words
@@ -115,6 +117,8 @@ __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
   o += w.bw;
   w.scr = o;
   o += 32;
+  w.touched = o;  // cells written by the current row (16 bits each)
+  o += kTouchCap / 2;
   w.score = o + 4;  // 4 words of margin below: the maxima scan reads 2 cycles early
   o += ncell + ncell / S + 12;
   o = (o + 1) & ~1;
@@ -133,8 +137,10 @@ __host__ __device__ inline size_t search_smem_bytes(int nw, int S, int h, int nc
   return (size_t)(kBlockHeaderWords + nw * warp_plan(S, h, ncell).total) * 4;
 }
 
+// Per-warp work counters (the statistics pass); 32 bits suffice for one warp's
+// share of a launch.
 struct Counters {
-  unsigned long long read = 0, acc = 0, off = 0, pairs = 0, bins1 = 0, frag = 0;
+  unsigned int read = 0, acc = 0, off = 0, pairs = 0, bins1 = 0, frag = 0;
 };
 
 // The rare case of add_chunk: lanes that hit the same cycle are grouped and summed
@@ -165,12 +171,18 @@ static __device__ __noinline__ void add_chunk_grouped(bool inc, int cell, int ad
 // Every accepted lane writes its lane number into its cycle's tag; a lane that
 // reads back another number shares the cycle, and only then are the lanes grouped
 // and summed by their lowest lane one rounded add at a time.
+// Accepted cells are also appended to `touched` (the next row clears them).
 __device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v, int lane,
                                           float* row, uint32_t* bm, uint32_t* tags, float* scr,
-                                          unsigned long long& n_acc) {
+                                          unsigned int& n_acc, uint16_t* touched, int& n_touched) {
   const unsigned act = __ballot_sync(kFull, inc);
   if (act == 0) return;
   n_acc += __popc(act);
+  if (inc) {
+    const int at = n_touched + __popc(act & ((1u << lane) - 1u));
+    if (at < kTouchCap) touched[at] = (uint16_t)cell;
+  }
+  n_touched += __popc(act);
   if (inc) tags[cell] = (uint32_t)lane;
   __syncwarp();
   const bool dup = inc && tags[cell] != (uint32_t)lane;
@@ -187,17 +199,18 @@ __device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v,
 }
 
 // Is `pos` the first entry of one of the bins (b0, b1)?  (slice_starts[b] == pos)
-__device__ __forceinline__ bool bin_starts_at(const uint32_t* ssw, uint32_t b0, uint32_t b1,
-                                              int64_t pos) {
+// Kept out of line: only entries at the window's first cycle ask.
+static __device__ __noinline__ bool bin_starts_at(const uint32_t* ssw, uint32_t b0, uint32_t b1,
+                                                  uint32_t pos) {
   uint32_t lo = b0 + 1, hi = b1;
   while (lo < hi) {
     const uint32_t mid = (lo + hi) >> 1;
-    if ((int64_t)__ldg(ssw + mid) < pos)
+    if (__ldg(ssw + mid) < pos)
       lo = mid + 1;
     else
       hi = mid;
   }
-  return lo < b1 && (int64_t)__ldg(ssw + lo) == pos;
+  return lo < b1 && __ldg(ssw + lo) == pos;
 }
 
 // fill_xic_slice for one (fragment, window) pair whose bin range [b0, b1) spans
@@ -214,78 +227,97 @@ struct ScanBatch {
   float v[kPrefetchChunks];
 };
 
-// Intensity of CSR entry i: f32, or (BF16 storage) the bfloat16 copy widened.
+// Entries of one observation: CSR positions are 32-bit offsets from its base.
+struct WinEntries {
+  const uint16_t* cy;
+  const float* in;
+  const uint16_t* in16;  // bfloat16 copy (BF16-storage searches)
+};
+
+__device__ __forceinline__ WinEntries win_entries(const SearchArgs& a, int64_t wbase) {
+  return WinEntries{a.cyc + wbase, a.inten + wbase, a.inten_bf16 + wbase};
+}
+
+// Intensity of entry q: f32, or (BF16 storage) the bfloat16 copy widened.
 template <bool FAST>
-__device__ __forceinline__ float ld_intensity(const SearchArgs& a, int64_t i) {
-  if (FAST) return __uint_as_float((uint32_t)__ldg(a.inten_bf16 + i) << 16);
-  return __ldg(a.inten + i);
+__device__ __forceinline__ float ld_intensity(const WinEntries& e, uint32_t q) {
+  if (FAST) return __uint_as_float((uint32_t)__ldg(e.in16 + q) << 16);
+  return __ldg(e.in + q);
 }
 
 template <bool FAST>
-__device__ __forceinline__ void load_batch(const SearchArgs& a, int64_t wbase, int64_t q0,
-                                           int64_t re, int lane, ScanBatch& b) {
+__device__ __forceinline__ void load_batch(const WinEntries& e, uint32_t q0, uint32_t re, int lane,
+                                           ScanBatch& b) {
 #pragma unroll
   for (int u = 0; u < kPrefetchChunks; ++u) {
-    const int64_t q = q0 + u * 32 + lane;
-    b.c[u] = q < re ? (int)__ldg(a.cyc + wbase + q) : -1;
-    b.v[u] = q < re ? ld_intensity<FAST>(a, wbase + q) : 0.0f;
+    const uint32_t q = q0 + u * 32 + lane;
+    b.c[u] = q < re ? (int)__ldg(e.cy + q) : -1;
+    b.v[u] = q < re ? ld_intensity<FAST>(e, q) : 0.0f;
   }
 }
 
-__device__ __forceinline__ bool scans(const SearchArgs& a, int64_t n) {
-  return a.gather_mode == 1 || (a.gather_mode == 0 && n <= a.scan_thresh);
+__device__ __forceinline__ bool scans(const SearchArgs& a, uint32_t n) {
+  return a.gather_mode == 1 || (a.gather_mode == 0 && n <= (uint32_t)a.scan_thresh);
 }
 
+// `pre`: the range's first batch, already loaded (or null).
 template <int S, bool FAST>
 __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64_t wbase,
-                                            uint32_t b0, uint32_t b1, int64_t rs, int64_t re,
+                                            uint32_t b0, uint32_t b1, uint32_t rs, uint32_t re,
                                             int cs, int ce, int lane, float* row, int off,
                                             uint32_t* bm, uint32_t* tags, float* scr,
-                                            Counters& k) {
-  const int64_t n = re - rs;
-  if (n <= 0) return;
-  const uint16_t* cy = a.cyc + wbase;
+                                            Counters& k, const ScanBatch* pre, uint16_t* touched,
+                                            int& n_touched) {
+  if (re <= rs) return;
+  const uint32_t n = re - rs;
+  const WinEntries e = win_entries(a, wbase);
   if (scans(a, n)) {
     k.read += n;
-    for (int64_t q0 = rs; q0 < re; q0 += 32 * kPrefetchChunks) {
+    for (uint32_t q0 = rs; q0 < re; q0 += 32 * kPrefetchChunks) {
       ScanBatch bt;
-      load_batch<FAST>(a, wbase, q0, re, lane, bt);
-      const int* c = bt.c;
-      const float* v = bt.v;
+      if (pre != nullptr && q0 == rs)
+        bt = *pre;
+      else
+        load_batch<FAST>(e, q0, re, lane, bt);
 #pragma unroll
       for (int u = 0; u < kPrefetchChunks; ++u) {
-        const int64_t qb = q0 + u * 32;
+        const uint32_t qb = q0 + u * 32;
         if (qb >= re) break;
-        const int64_t q = qb + lane;
-        const int cu = c[u];
-        int nxt = __shfl_down_sync(kFull, cu, 1);
-        const int nxt_first = __shfl_sync(kFull, c[u + 1 < kPrefetchChunks ? u + 1 : u], 0);
-        if (lane == 31) nxt = (u + 1 < kPrefetchChunks) ? nxt_first : -2;
+        const uint32_t q = qb + lane;
+        const int cu = bt.c[u];
         bool inc = q < re && cu > cs && cu < ce;
-        if (q < re && cu == cs) {
-          const int64_t qn = q + 1;
-          bool last = qn >= re;
-          if (!last) last = bin_starts_at(a.ss + a.win[wsel].ss_off, b0, b1, qn);
-          if (!last) {
-            const int cn = nxt == -2 ? (int)__ldg(cy + qn) : nxt;
-            last = cn != cs;
+        const bool at_start = q < re && cu == cs;
+        if (__any_sync(kFull, at_start)) {
+          int nxt = __shfl_down_sync(kFull, cu, 1);
+          const int nxt_first = __shfl_sync(kFull, bt.c[u + 1 < kPrefetchChunks ? u + 1 : u], 0);
+          if (lane == 31) nxt = (u + 1 < kPrefetchChunks) ? nxt_first : -2;
+          if (at_start) {
+            const uint32_t qn = q + 1;
+            bool last = qn >= re;
+            if (!last) last = bin_starts_at(a.ss + a.win[wsel].ss_off, b0, b1, qn);
+            if (!last) {
+              const int cn = nxt == -2 ? (int)__ldg(e.cy + qn) : nxt;
+              last = cn != cs;
+            }
+            inc = last;
           }
-          inc = last;
         }
         const int cell = cu - cs;
-        add_chunk(inc, cell, inc ? raddr<S>(cell + off) : 0, v[u], lane, row, bm, tags, scr, k.acc);
+        add_chunk(inc, cell, inc ? raddr<S>(cell + off) : 0, bt.v[u], lane, row, bm, tags, scr,
+                  k.acc, touched, n_touched);
       }
     }
   } else {
     const uint32_t* ssw = a.ss + a.win[wsel].ss_off;
+    const uint16_t* cy = e.cy;
     for (uint32_t bb = b0; bb < b1; bb += 32) {
       const uint32_t b = bb + lane;
       const bool vb = b < b1;
       int64_t pos = 0, cnt = 0;
       if (vb) {
-        const int64_t s = __ldg(ssw + b), e = __ldg(ssw + b + 1);
-        pos = s + rust_bsearch_u16(cy + s, e - s, cs);
-        const int64_t end = pos + lower_bound_u16(cy + pos, e - pos, ce);
+        const int64_t s0 = __ldg(ssw + b), s1 = __ldg(ssw + b + 1);
+        pos = s0 + rust_bsearch_u16(cy + s0, s1 - s0, cs);
+        const int64_t end = pos + lower_bound_u16(cy + pos, s1 - pos, ce);
         cnt = end - pos;
       }
       k.off += 2 * __popc(__ballot_sync(kFull, vb));
@@ -312,9 +344,10 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
         const bool vt = t < total;
         const int64_t q = opos + (t - oex);
         const int c = vt ? (int)__ldg(cy + q) : 0;
-        const float v = vt ? ld_intensity<FAST>(a, wbase + q) : 0.0f;
+        const float v = vt ? ld_intensity<FAST>(e, (uint32_t)q) : 0.0f;
         const int cell = c - cs;
-        add_chunk(vt, cell, vt ? raddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, k.acc);
+        add_chunk(vt, cell, vt ? raddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, k.acc,
+                  touched, n_touched);
       }
     }
   }
@@ -436,20 +469,20 @@ __device__ __forceinline__ void cmpx(float& v, int& i, int j, bool keep_best) {
 
 // Bitonic sort of one key per lane, best in lane 0.
 __device__ __forceinline__ void warp_sort_best_first(float& v, int& i, int lane) {
-#pragma unroll
+#pragma unroll 1
   for (int k = 2; k <= 32; k <<= 1)
-#pragma unroll
+#pragma unroll 1
     for (int j = k >> 1; j > 0; j >>= 1) cmpx(v, i, j, ((lane & j) == 0) == ((lane & k) == 0));
 }
 
 // Sorts a bitonic sequence across the lanes, best in lane 0.
 __device__ __forceinline__ void warp_merge_best_first(float& v, int& i, int lane) {
-#pragma unroll
+#pragma unroll 1
   for (int j = 16; j > 0; j >>= 1) cmpx(v, i, j, (lane & j) == 0);
 }
 
 template <int H, int S, bool FAST>
-__global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
+__global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
   extern __shared__ __align__(16) float smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int h = H > 0 ? H : a.h;
@@ -464,6 +497,13 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
   float* score = wb + P.score;
   float* mval = wb + P.mval;
   int* midx = reinterpret_cast<int*>(wb + P.midx);
+  uint16_t* touched = reinterpret_cast<uint16_t*>(wb + P.touched);
+  int n_touched = 0;  // cells the last row wrote (warp-uniform)
+  {
+    float4* r4 = reinterpret_cast<float4*>(row);
+    for (int i = lane; i < P.row_words / 4; i += 32) r4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = lane; i < P.bw; i += 32) bm[i] = 0u;
+  }
 
   for (int i = threadIdx.x; i < kLnTableSize; i += blockDim.x) lnt[i] = a.ln_tab[i];
   for (int i = threadIdx.x; i <= a.h; i += blockDim.x) kw_s[i] = a.kw[i];
@@ -506,15 +546,27 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
     uint32_t rs = 0, re = 0, b0 = 0, b1 = 0;
     int wsel = 0;
     int64_t wbase = 0;
+    // the first batch of the next fragment's first pair, loaded while this
+    // fragment's row is convolved
+    ScanBatch pre;
+    int pre_pi = -1;
     for (int f = 0; f < F; ++f) {
-      {
+      // the previous row's cells (and bitmap words) back to zero
+      if (n_touched > kTouchCap) {
         float4* r4 = reinterpret_cast<float4*>(row);
         for (int i = lane; i < P.row_words / 4; i += 32) r4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         for (int i = lane; i < P.bw; i += 32) bm[i] = 0u;
+      } else {
+        for (int i = lane; i < n_touched; i += 32) {
+          const int c = touched[i];
+          row[raddr<S>(c + P.off)] = 0.0f;
+          bm[(c + kBitOff) >> 5] = 0u;
+        }
       }
+      n_touched = 0;
       __syncwarp();
       // ---- 1. gather: the fragment's pairs in window order
-      const unsigned long long acc0 = k.acc;
+      const unsigned int acc0 = k.acc;
       for (int wi = 0; wi < nwin; ++wi) {
         const int pi = f * nwin + wi;
         if (pi >= pb + 32) {
@@ -550,9 +602,23 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
         k.pairs += 1;
         k.bins1 += qb1 - qb0 + 1;
         gather_pair<S, FAST>(a, qw, qbase, qb0, qb1, qrs, qre, cs, ce, lane, row, P.off, bm, tags,
-                             scr, k);
+                             scr, k, pi == pre_pi ? &pre : nullptr, touched, n_touched);
       }
       __syncwarp();
+      {
+        const int pn = (f + 1) * nwin;
+        pre_pi = -1;
+        if (pn < npairs && pn < pb + 32) {
+          const int q = pn - pb;
+          const uint32_t nrs = __shfl_sync(kFull, rs, q), nre = __shfl_sync(kFull, re, q);
+          const uint32_t nb0 = __shfl_sync(kFull, b0, q), nb1 = __shfl_sync(kFull, b1, q);
+          const int64_t nbase = __shfl_sync(kFull, wbase, q);
+          if (nb1 > nb0 && nre > nrs && scans(a, nre - nrs)) {
+            load_batch<FAST>(win_entries(a, nbase), nrs, nre, lane, pre);
+            pre_pi = pn;
+          }
+        }
+      }
       float wf = __shfl_sync(kFull, wf_lane, f & 31);
       if (f >= 32) wf = __ldg(a.fw + p * a.kf + f);
       if (!isfinite(wf)) {
@@ -760,11 +826,11 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchArgs a) {
     if (lane == 0) a.cand_n[p] = kk;
   }
   if (a.stats && lane == 0) {
-    atomicAdd(a.stats + 0, k.pairs);
-    atomicAdd(a.stats + 1, k.bins1);
-    atomicAdd(a.stats + 2, k.frag);
-    atomicAdd(a.stats + 3, k.read);
-    atomicAdd(a.stats + 4, k.acc);
-    atomicAdd(a.stats + 5, k.off);
+    atomicAdd(a.stats + 0, (unsigned long long)k.pairs);
+    atomicAdd(a.stats + 1, (unsigned long long)k.bins1);
+    atomicAdd(a.stats + 2, (unsigned long long)k.frag);
+    atomicAdd(a.stats + 3, (unsigned long long)k.read);
+    atomicAdd(a.stats + 4, (unsigned long long)k.acc);
+    atomicAdd(a.stats + 5, (unsigned long long)k.off);
   }
 }
