@@ -320,9 +320,17 @@ def library_arrays(lib: dict) -> dict:
 
 # -------------------------------------------------------------------- run
 
+# Random MS2 peaks generated and sorted at once by the torch backend; larger runs
+# are generated in blocks of consecutive cycles (the sort of ~1e9 float64 keys with
+# its index arrays is what bounds device memory).
+TORCH_BLOCK_PEAKS = 1_200_000_000
+
+
 def make_run(cfg: SynthConfig, lib: dict, backend="numpy", device="cuda:0") -> dict:
     """DIA run arrays in the argument order of DIAData.from_arrays (on the
     backend's device); ``cycle`` is a host array."""
+    if backend == "torch" and cfg.n_ms2_peaks > TORCH_BLOCK_PEAKS:
+        return _make_run_torch_blocked(cfg, lib, device)
     B = _backend(backend, cfg.seed * 104729 + 7, device)
     W, NC, N = cfg.n_windows, cfg.n_cycles, cfg.peaks_per_spectrum
     n_spec = NC * (W + 1)
@@ -422,6 +430,115 @@ def make_run(cfg: SynthConfig, lib: dict, backend="numpy", device="cuda:0") -> d
                 spectrum_peak_start_idx=B.i64(start), spectrum_peak_stop_idx=B.i64(stop),
                 spectrum_cycle_idx=B.i64(cyc), spectrum_rt=rt, peak_mz=peak_mz, peak_intensity=peak_int,
                 cycle=cycle_arr)
+
+
+def _make_run_torch_blocked(cfg: SynthConfig, lib: dict, device: str) -> dict:
+    """make_run for runs too large to generate at once (torch backend): the same
+    distributions, with the planted peaks drawn first and the random peaks drawn,
+    merged and sorted one block of consecutive cycles at a time, each block written
+    into the preallocated peak arrays.  Only the block being sorted holds float64
+    keys, so device memory stays near the size of the final f32 arrays."""
+    import torch
+
+    B = _TORCH(cfg.seed * 104729 + 11, device)
+    t = torch
+    dev = B.dev
+    W, NC, N = cfg.n_windows, cfg.n_cycles, cfg.peaks_per_spectrum
+    S1 = W + 1
+    n_spec = NC * S1
+    sidx = t.arange(n_spec, device=dev)
+    cyc = sidx // S1
+    dsi = sidx % S1
+    wlo = cfg.window_start + (dsi - 1).clamp(min=0) * cfg.window_width
+    ms1 = dsi == 0
+    iso_lo = wlo.to(t.float32).masked_fill(ms1, -1.0)
+    iso_hi = (wlo + cfg.window_width).to(t.float32).masked_fill(ms1, -1.0)
+    rt = cyc.to(t.float64).to(t.float32)
+    del sidx, wlo
+
+    # planted peaks (spectrum id, m/z, intensity), all cycles at once
+    planted = lib["planted"].to(dev)
+    apex = lib["apex"].to(dev)
+    pmz = lib["precursor_mz"].to(dev)
+    fst = lib["flat_frag_start_idx"].to(dev)
+    fsp = lib["flat_frag_stop_idx"].to(dev)
+    fmz_all = lib["fragment_mz"].to(dev)
+    fint_all = lib["fragment_intensity"].to(dev)
+    pl_ids = t.arange(planted.shape[0], device=dev)[planted]
+    half = int(np.ceil(4 * PLANT_SIGMA))
+    span = 2 * half + 1
+    nfr = (fsp - fst)[pl_ids]
+    pf_prec = t.repeat_interleave(pl_ids, nfr)
+    first = t.cumsum(nfr, 0) - nfr
+    pf_frag = fst[pf_prec] + (t.arange(pf_prec.shape[0], device=dev) - t.repeat_interleave(first, nfr))
+    pm = pmz[pf_prec]
+    w_a = ((pm.to(t.float64) - cfg.window_start) / cfg.window_width).floor().to(t.int64) + 1
+    p_spec, p_mz, p_int = [], [], []
+    for dw in (0, -1):
+        w = w_a + dw
+        wc = w.clamp(1, W)
+        lo_w = (cfg.window_start + (wc - 1) * cfg.window_width).to(t.float32)
+        hi_w = (cfg.window_start + (wc - 1) * cfg.window_width + cfg.window_width).to(t.float32)
+        ok = (w >= 1) & (w <= W) & (lo_w <= pm) & (hi_w >= pm)
+        sel = t.nonzero(ok).flatten()
+        if sel.numel() == 0:
+            continue
+        rep = t.repeat_interleave(sel, span)
+        off = (t.arange(rep.numel(), device=dev) % span) - half
+        ap = apex[pf_prec[rep]]
+        c = ap.round().to(t.int64) + off
+        good = (c >= 0) & (c < NC)
+        rep, c, ap = rep[good], c[good], ap[good]
+        frag = pf_frag[rep]
+        d = c.to(t.float64) - ap
+        inten = PLANT_AMPLITUDE * fint_all[frag].to(t.float64) * t.exp(-(d * d) / (2 * PLANT_SIGMA ** 2)) * \
+            t.exp(PLANT_NOISE_SIGMA * B.randn(rep.numel()))
+        mzj = fmz_all[frag].to(t.float64) * (1.0 + PLANT_PPM_JITTER * 1e-6 * B.randn(rep.numel()))
+        p_spec.append(c * S1 + wc[rep])
+        p_mz.append(mzj.to(t.float32))
+        p_int.append(inten.to(t.float32))
+        del rep, off, ap, c, good, frag, d, inten, mzj
+    p_spec = t.cat(p_spec) if p_spec else t.zeros(0, dtype=t.int64, device=dev)
+    p_mz = t.cat(p_mz) if p_mz else t.zeros(0, dtype=t.float32, device=dev)
+    p_int = t.cat(p_int) if p_int else t.zeros(0, dtype=t.float32, device=dev)
+    del pf_prec, pf_frag, pm, w_a, first, nfr, pl_ids
+
+    counts = t.bincount(p_spec, minlength=n_spec).to(t.int64)
+    counts[~ms1] += N
+    stop = t.cumsum(counts, 0)
+    start = stop - counts
+    total = int(stop[-1].item()) if n_spec else 0
+    peak_mz = t.empty(total, dtype=t.float32, device=dev)
+    peak_int = t.empty(total, dtype=t.float32, device=dev)
+
+    # blocks of consecutive cycles: their spectra, and so their peaks, are contiguous
+    cyc_per_block = max(1, TORCH_BLOCK_PEAKS // max(1, W * N))
+    p_cyc = p_spec // S1
+    for c0 in range(0, NC, cyc_per_block):
+        c1 = min(NC, c0 + cyc_per_block)
+        s0, s1 = c0 * S1, c1 * S1
+        ms2_ids = t.arange(s0, s1, device=dev)
+        ms2_ids = ms2_ids[(ms2_ids % S1) != 0]
+        n_rand = ms2_ids.numel() * N
+        r_spec = t.repeat_interleave(ms2_ids, N)
+        r_mz = (PEAK_MZ_RANGE[0] + (PEAK_MZ_RANGE[1] - PEAK_MZ_RANGE[0]) * B.rand(n_rand)).to(t.float32)
+        r_int = t.exp(8.0 + 2.0 * B.randn(n_rand)).to(t.float32)
+        sel = t.nonzero((p_cyc >= c0) & (p_cyc < c1)).flatten()
+        spec = t.cat([r_spec, p_spec[sel]])
+        mz = t.cat([r_mz, p_mz[sel]])
+        inten = t.cat([r_int, p_int[sel]])
+        del r_spec, r_mz, r_int, ms2_ids, sel
+        key = (spec - s0).to(t.float64) * 2048.0 + mz.to(t.float64)
+        order = t.sort(key, stable=True).indices
+        del key, spec
+        o0 = int(start[s0].item())
+        peak_mz[o0:o0 + order.numel()] = mz[order]
+        peak_int[o0:o0 + order.numel()] = inten[order]
+        del order, mz, inten
+    cycle_arr = np.zeros((W + 1, 1, 1, 1), np.float32)
+    return dict(spectrum_delta_scan_idx=dsi, isolation_lower_mz=iso_lo, isolation_upper_mz=iso_hi,
+                spectrum_peak_start_idx=start, spectrum_peak_stop_idx=stop, spectrum_cycle_idx=cyc,
+                spectrum_rt=rt, peak_mz=peak_mz, peak_intensity=peak_int, cycle=cycle_arr)
 
 
 def run_to_numpy(run: dict) -> dict:

@@ -47,8 +47,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg1")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-windows", type=int, default=24,
-                    help="MS2 windows in the CPU-baseline sample")
+    ap.add_argument("--cpu-windows", type=int, default=0,
+                    help="MS2 windows in the CPU-baseline sample (0: about 72 M peaks' worth)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warps-per-block", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
@@ -149,6 +149,10 @@ def make_device_workload(name: str, device: str, lib_seed_offset: int = 0):
     lib_cfg = synth.get_config(name, seed=cfg.seed + 1000 * lib_seed_offset) if lib_seed_offset else cfg
     lib = synth.make_library(lib_cfg, "torch", device)
     run = synth.make_run(cfg, lib, "torch", device)
+    import torch
+
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()  # the generator's temporaries: the engine allocates outside torch
     return cfg, lib, run
 
 
@@ -179,6 +183,15 @@ def library_tensors(lib: dict, device: str):
     if lib.get("rt_tolerance") is not None:
         out["precursor_rt_tolerance"] = lib["rt_tolerance"].contiguous()
     return out
+
+
+def sample_windows(cfg, requested: int) -> int:
+    """MS2 windows of the CPU sample: as requested, else about 72 M peaks' worth
+    (24 windows at 3000 cycles x 1000 peaks)."""
+    if requested > 0:
+        return min(requested, cfg.n_windows)
+    per_window = cfg.n_cycles * cfg.peaks_per_spectrum
+    return max(1, min(cfg.n_windows, round(72e6 / per_window)))
 
 
 def window_subset(cfg, run: dict, lib: dict, n_windows: int):
@@ -316,7 +329,7 @@ def run_reference(args, rank, world):
 
     device = "cuda:0"
     cfg, lib, run = make_device_workload(args.workload, device)
-    host, sub, (w0, w1) = window_subset(cfg, run, lib, args.cpu_windows)
+    host, sub, (w0, w1) = window_subset(cfg, run, lib, sample_windows(cfg, args.cpu_windows))
     del run
     torch.cuda.empty_cache()
     n = cpu_threads()
@@ -513,7 +526,7 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         import oracle
 
-        host, sub, (w0, w1) = window_subset(cfg, run, lib, args.cpu_windows)
+        host, sub, (w0, w1) = window_subset(cfg, run, lib, sample_windows(cfg, args.cpu_windows))
         n = cpu_threads()
         od, ol, tol = oracle_setup(host, sub, n)
         ts, res = time_oracle(od, ol, tol, cfg.params_dict(), n, steps=3, warmup=1)

@@ -238,7 +238,10 @@ class Dia:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().orc_dia_free(self._h)
+            try:
+                lib().orc_dia_free(self._h)
+            except TypeError:  # interpreter shutdown: module globals already cleared
+                pass
             self._h = None
 
     @property
@@ -323,7 +326,10 @@ class Lib:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().orc_lib_free(self._h)
+            try:
+                lib().orc_lib_free(self._h)
+            except TypeError:  # interpreter shutdown: module globals already cleared
+                pass
             self._h = None
 
 
