@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--warps-per-block", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--cycles-per-lane", type=int, default=0)
+    ap.add_argument("--gather-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="0 automatic, 1 scan every bin range, 2 binary-search every bin")
     ap.add_argument("--graph", action="store_true",
                     help="replay a captured CUDA graph per search (stage times then come "
                          "from a second, directly enqueued pass)")
@@ -406,7 +408,7 @@ def run_ours(args, rank, world, local_rank):
                                  precision=precision, use_graph=args.graph,
                                  warps_per_block=args.warps_per_block,
                                  cycles_per_lane=args.cycles_per_lane,
-                                 blocks_per_sm=args.blocks_per_sm)
+                                 blocks_per_sm=args.blocks_per_sm, gather_mode=args.gather_mode)
     tuned = sel.autotune(dia, slib) if args.autotune else None
     sel_opts = ((tuned["warps_per_block"], tuned["cycles_per_lane"]) if tuned
                 else (args.warps_per_block, args.cycles_per_lane))
@@ -448,7 +450,8 @@ def run_ours(args, rank, world, local_rank):
         sel_st = ads.PeakGroupSelection(params, verbose=False, device=local_rank, time_stages=True,
                                         precision=precision, warps_per_block=sel_opts[0],
                                         cycles_per_lane=sel_opts[1],
-                                        blocks_per_sm=args.blocks_per_sm)
+                                        blocks_per_sm=args.blocks_per_sm,
+                                        gather_mode=args.gather_mode)
         cand_st = sel_st.new_candidates()
         for _ in range(args.warmup):
             sel_st.search_into(dia, slib, cand_st)
@@ -563,6 +566,7 @@ def run_ours(args, rank, world, local_rank):
                    "peaks": n_peaks_total, "candidates_per_step": int(n_cand),
                    "precursors_per_gpu": int(P), "parallelism": f"replicated run, {world} library shard(s)",
                    "launch": {"cuda_graph": bool(args.graph), "autotuned": tuned,
+                              "gather_mode": args.gather_mode,
                               "warps_per_block": sel_opts[0] or "default",
                               "cycles_per_lane": sel_opts[1] or "length classes"}},
         "e2e": {"value": e2e_value, "unit": "precursors/s", "h2d_bytes_per_step": int(h2d),
