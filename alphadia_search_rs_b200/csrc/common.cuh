@@ -212,8 +212,8 @@ std::vector<double2> host_ln_table();  // the values device_ln_table uploads
 
 // The same value as ln_rn(x) for every float x, computed faster: x = 2^e * m,
 // m = c_j * (1 + r) with 0 <= r < 2^-8, ln(1 + r) by its Taylor series to r^5,
-// all in double; every term is non-negative for x > 1, so the result y carries a
-// relative error below 2^-42.  Rounding y to float is then correct unless the 29
+// all in double; e*ln2 + ln(c_j) and r*p(r) are non-negative for x > 1, so the
+// result y carries a relative error below 2^-42.  Rounding y to float is then correct unless the 29
 // bits of y's significand below float precision lie within 2^14 units of the
 // halfway pattern (about one input in 2^14); there ln_rn decides.  Checked against
 // ln_rn for every float in (1, inf).  `tab` is the table of device_ln_table
@@ -228,13 +228,14 @@ __device__ __forceinline__ float ln_fast(float x, const double2* tab, bool* slow
   const double m = (double)__uint_as_float((b & 0x007FFFFFu) | 0x3F800000u);
   const double2 t = tab[j];
   const double r = fma(m, t.x, -1.0);
-  double p = 1.0 / 5.0;
-  p = fma(p, r, -1.0 / 4.0);
-  p = fma(p, r, 1.0 / 3.0);
-  p = fma(p, r, -1.0 / 2.0);
-  p = fma(p, r, 1.0);
+  // 1 - r/2 + r^2/3 - r^3/4 + r^4/5 as (1 - r/2) + r^2 * ((1/3 - r/4) + r^2/5): three
+  // dependent steps after r instead of four; e*ln2 + ln(c_j) forms alongside
+  const double r2 = r * r;
+  const double c0 = fma(r, -1.0 / 2.0, 1.0);
+  const double c1 = fma(r, -1.0 / 4.0, 1.0 / 3.0);
+  const double p = fma(r2, fma(r2, 1.0 / 5.0, c1), c0);
   const double ln2 = 0.6931471805599453094172321;
-  const double y = fma((double)e, ln2, fma(p, r, t.y));
+  const double y = fma(p, r, fma((double)e, ln2, t.y));
   const uint32_t low = (uint32_t)__double2loint(y) & 0x1FFFFFFFu;
   if (low - (0x10000000u - 0x4000u) < 0x8000u) {
     if (slow) *slow = true;
