@@ -253,6 +253,27 @@ def window_subset(cfg, run: dict, lib: dict, n_windows: int):
     return host, sub, (w0, w1)
 
 
+def bf16_agreement(got: dict, ref: dict, eps_rel_max: float = 1e-3):
+    """(fraction of the FP64 oracle's (precursor, rank) rows whose cycle the GPU
+    found too, relative score errors over those rows).  The error of a row is taken
+    against max(|s64|, eps_rel_max * the precursor's largest |s64|), since scores
+    near zero are common at the RT-window edges."""
+    ref_max = {}
+    for p, s64 in zip(ref["precursor_idx"], ref["score_f64"]):
+        ref_max[int(p)] = max(ref_max.get(int(p), 0.0), abs(float(s64)))
+    mine = {(int(p), int(r)): (int(c), float(s)) for p, r, c, s in
+            zip(got["precursor_idx"], got["rank"], got["cycle_center"], got["score"])}
+    same, errs = 0, []
+    for p, r, c, s64 in zip(ref["precursor_idx"], ref["rank"], ref["cycle_center"], ref["score_f64"]):
+        m = mine.get((int(p), int(r)))
+        if m is None or m[0] != int(c):
+            continue
+        same += 1
+        den = max(abs(float(s64)), eps_rel_max * ref_max[int(p)])
+        errs.append(abs(m[1] - float(s64)) / den if den > 0 else 0.0)
+    return same / max(len(ref["rank"]), 1), np.asarray(errs if errs else [0.0])
+
+
 def oracle_setup(host: dict, sub: dict, n_threads: int):
     import oracle
 
@@ -551,6 +572,19 @@ def run_ours(args, rank, world, local_rank):
         parity = {"precursors": int(len(sub["precursor_idx"])), "candidates": int(len(res["rank"])),
                   "indices_identical": all(same.values()) and int(mask.sum()) == len(res["rank"]),
                   "max_score_rel_err_vs_glibc_logf": rel}
+        if precision == "bf16":
+            # BF16 storage is compared with the FP64 oracle: top-K cycle agreement and
+            # relative score error (against max(|s64|, 1e-3 * the precursor's largest |s64|))
+            ref64 = oracle.search(od, ol, oracle.Params(**cfg.params_dict()),
+                                  rt_tolerance_per_precursor=tol, log_mode=oracle.LOG_RN,
+                                  precision=1, n_threads=n)
+            agree, errs = bf16_agreement({k: v[mask] for k, v in got.items()}, ref64)
+            parity = {"precursors": int(len(sub["precursor_idx"])),
+                      "candidates_fp64_oracle": int(len(ref64["rank"])),
+                      "topk_cycle_agreement_vs_fp64": agree,
+                      "score_rel_err_vs_fp64_max": float(errs.max()),
+                      "score_rel_err_vs_fp64_p99": float(np.quantile(errs, 0.99)),
+                      "score_rel_err_vs_fp64_median": float(np.median(errs))}
 
     line = {
         "metric": METRIC, "value": value, "unit": "precursors/s", "n_gpus": world,
