@@ -81,6 +81,11 @@ CONFIGS = {
                         (40.0, 40.0), 15.0, 2.0, 21, 3, 12, seed=11),
     "tiny_uneven": SynthConfig("tiny_uneven", 400, 6, 10.0, 400.0, 400, 600, 4, 24, (400.0, 460.0),
                                (2, 4), (30.0, 160.0), 15.0, 2.0, 21, 3, 24, decoy_fraction=0.5, seed=12),
+    # cfg4's search settings (kernel sigma 3 / width 31, 10 ppm, top-5, 4-24 fragments,
+    # RT half-windows up to 300 cycles: several length classes, multi-pass rows)
+    "tiny_cfg4": SynthConfig("tiny_cfg4", 700, 6, 8.0, 400.0, 400, 400, 4, 24, (400.0, 448.0),
+                             (2, 4), (30.0, 300.0), 10.0, 3.0, 31, 5, 24, decoy_fraction=0.5,
+                             seed=13),
     # the benchmark configurations
     "cfg0": SynthConfig("cfg0", 1000, 8, 25.0, 400.0, 1500, 2000, 12, 12, (400.0, 600.0), (2, 3),
                         (100.0, 100.0), 15.0, 2.0, 21, 3, 12, seed=100),

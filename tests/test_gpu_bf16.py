@@ -46,7 +46,8 @@ def compare_to_fp64(got: dict, ref: dict):
     return same / max(len(ref["rank"]), 1), np.asarray(errs if errs else [0.0])
 
 
-@pytest.mark.parametrize("name,min_agree", [("tiny", 0.99), ("tiny_uneven", 0.99), ("cfg0", 0.995)])
+@pytest.mark.parametrize("name,min_agree", [("tiny", 0.99), ("tiny_uneven", 0.99), ("tiny_cfg4", 0.99),
+                                            ("cfg0", 0.995)])
 def test_bf16_against_fp64_oracle(name, min_agree):
     cfg, lib, run = synth.make_workload(name, "numpy")
     la = synth.library_arrays(lib)
