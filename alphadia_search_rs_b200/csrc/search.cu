@@ -299,7 +299,8 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a) {
 // unrolled stencils for the half widths of kernel_size 20, 21-22 and 31-32, any
 // other half width through the generic path.
 constexpr int kLaneCycles[] = {4, 8, 10, 12, 16};
-constexpr int kMaxClasses = 6;
+constexpr int kDefaultWarpsPerBlock = 4;
+constexpr int kMaxClasses = 10;
 
 // Length classes of one search: class b covers C <= bound[b] with S[b] cycles per
 // lane (bound[last] = the longest window, searched in one or more passes).
@@ -308,31 +309,44 @@ struct LenClasses {
   int S[kMaxClasses];
 };
 
-// The fewest lane slots (passes * 32 * S) covering c cycles, ties to the larger S.
+// Relative cost of searching a c-cycle window with S cycles per lane: passes times
+// (S outputs + about 6 outputs' worth of per-pass loads and control per lane).
+int lane_cost(int64_t c, int S) { return (int)((c + 32 * S - 1) / (32 * S)) * (S + 6); }
+
+// The cheapest lane width for a c-cycle window, ties to the larger S.
 int best_lane_cycles(int64_t c) {
   int S = kLaneCycles[0];
-  int64_t best = -1;
+  int best = -1;
   for (int cand : kLaneCycles) {
-    const int64_t slots = (c + 32 * cand - 1) / (32 * cand) * 32 * cand;
-    if (best < 0 || slots <= best) {
-      best = slots;
+    const int cost = lane_cost(c, cand);
+    if (best < 0 || cost <= best) {
+      best = cost;
       S = cand;
     }
   }
   return S;
 }
 
-// One class per lane width whose single pass is shorter than the longest window,
-// then one for the rest.  A fixed cycles_per_lane gives a single class.
+// Length classes: every bound 32 * S * k (k <= 4 passes) below the longest window, at
+// least 20 % apart, each with its cheapest lane width, then one class for the rest.
+// A fixed cycles_per_lane gives a single class.
 int plan_classes(int64_t c_max, int fixed_S, LenClasses* out) {
   int n = 0;
   if (fixed_S == 0) {
-    for (int s : kLaneCycles)
-      if (32 * (int64_t)s < c_max) {
-        out->bound[n] = 32 * s;
-        out->S[n] = s;
-        ++n;
-      }
+    std::vector<int> bounds;
+    for (int S : kLaneCycles)
+      for (int k = 1; k <= 4; ++k)
+        if ((int64_t)32 * S * k < c_max) bounds.push_back(32 * S * k);
+    std::sort(bounds.begin(), bounds.end());
+    int last = 0;
+    for (int b : bounds) {
+      if (n == kMaxClasses - 1) break;
+      if (last > 0 && (int64_t)b * 5 < (int64_t)last * 6) continue;
+      out->bound[n] = b;
+      out->S[n] = best_lane_cycles(b);
+      last = b;
+      ++n;
+    }
   }
   out->bound[n] = (int)c_max;
   out->S[n] = fixed_S ? fixed_S : best_lane_cycles(c_max);
@@ -821,8 +835,9 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     const int S = cls.S[b];
     const int cmax_b = cls.bound[b];
     const int ncell_b = (cmax_b + 32 * S - 1) / (32 * S) * 32 * S;
-    // block shape: warps per block (one precursor per warp at a time)
-    int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : 8;
+    // block shape: warps per block (one precursor per warp at a time); 4 by default,
+    // which packs long-window classes into shared memory better than 8
+    int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : kDefaultWarpsPerBlock;
     nw = std::max(1, std::min(nw, 8));
     while (nw > 1 && search_smem_bytes(nw, S, s->h, ncell_b) > (size_t)max_smem) --nw;
     const size_t smem = search_smem_bytes(nw, S, s->h, ncell_b);
@@ -1346,15 +1361,7 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   if (c_max > kMaxCycles)
     return fail(ADS_ERR_INVALID_ARGUMENT, "RT windows longer than 2048 cycles are not supported (" +
                                               std::to_string(c_max) + " cycles)");
-  int S = kLaneCycles[0];
-  int64_t best = -1;
-  for (int cand : kLaneCycles) {
-    const int64_t slots = (c_max + 32 * cand - 1) / (32 * cand) * 32 * cand;
-    if (best < 0 || slots <= best) {
-      best = slots;
-      S = cand;
-    }
-  }
+  const int S = best_lane_cycles(c_max);
   const int ncell = (int)((c_max + 32 * S - 1) / (32 * S) * 32 * S);
   const int k_out = (int)std::max<int64_t>(0, std::min<int64_t>(prm.candidate_count, maxima_cap(ncell)));
   const int kf = (int)std::max<int64_t>(1, std::min<int64_t>(prm.top_k_fragments, l->max_frag));
@@ -1444,7 +1451,7 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   prep_kernel<<<(int)prep_blocks, kPrepThreads, 0, st>>>(pa);
   ADS_LAUNCH_CHECK();
 
-  int nw = 8;
+  int nw = kDefaultWarpsPerBlock;
   int max_smem = 0;
   ADS_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
   while (nw > 1 && search_smem_bytes(nw, S, h, ncell) > (size_t)max_smem) --nw;

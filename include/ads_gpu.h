@@ -162,7 +162,7 @@ typedef struct {
   int32_t verbose;     /* 1: print the reference's two lines after each search
                           (src/peak_group_selection/mod.rs:123-125) */
   int32_t use_graph;   /* 1: capture the search pipeline in a CUDA graph and replay it */
-  int32_t warps_per_block; /* 0 = autotuned/default */
+  int32_t warps_per_block; /* 0 = default (4); else 1..8 warps, one precursor each */
   int32_t blocks_per_sm;   /* 0 = autotuned/default */
   int32_t gather_mode;     /* 0 = automatic, 1 = always scan bin ranges, 2 = always
                               binary-search each bin (both are exact; for testing) */
