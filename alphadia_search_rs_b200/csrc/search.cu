@@ -64,19 +64,21 @@ __device__ __forceinline__ int64_t lower_bound_u16(const uint16_t* a, int64_t n,
 
 // Same Rust search on the RT index (binary_search_by with partial_cmp,
 // src/rt_index/mod.rs:123-135).
+// `a` may be in shared or global memory (plain loads).
 __device__ __forceinline__ int rust_bsearch_f32(const float* a, int n, float x) {
   int size = n, base = 0;
   while (size > 1) {
     const int half = size / 2, mid = base + half;
-    base = (__ldg(a + mid) > x) ? base : mid;
+    base = (a[mid] > x) ? base : mid;
     size -= half;
   }
-  const float v = __ldg(a + base);
+  const float v = a[base];
   if (v == x) return base;
   return base + (v < x ? 1 : 0);
 }
 
-// RTIndex::get_cycle_idx_limits (src/rt_index/mod.rs:89-138).
+// RTIndex::get_cycle_idx_limits (src/rt_index/mod.rs:89-138).  `rt` may be in shared or
+// global memory.
 __device__ __forceinline__ void rt_limits(const float* rt, int n, float dt, float prt, float tol,
                                           float pad, int* lo, int* hi) {
   if (n == 0) {
@@ -87,7 +89,7 @@ __device__ __forceinline__ void rt_limits(const float* rt, int n, float dt, floa
   const float min_tol = __fmul_rn(__fadd_rn(10.0f, pad), dt);
   const float eff = fmaxf(tol, min_tol);
   const float lower = __fsub_rn(prt, eff), upper = __fadd_rn(prt, eff);
-  const float r0 = __ldg(rt), rn = __ldg(rt + n - 1);
+  const float r0 = rt[0], rn = rt[n - 1];
   if (upper < r0) {
     *lo = 0;
     *hi = 0;
@@ -145,7 +147,22 @@ struct PrepArgs {
   uint32_t* blo;
   uint32_t* bhi;
   int* err;
+  int win_in_smem;  // stage the isolation windows / the RT index in shared memory
+  int rt_in_smem;
 };
+
+// Shared memory of a prep block: the isolation windows, then the MS1 retention times,
+// each when it fits the 48 KB a block gets without opting in.
+constexpr size_t kPrepSmemBytes = 48 * 1024;
+
+__host__ __device__ inline size_t prep_win_bytes(int n_obs) { return ((size_t)n_obs * sizeof(WinInfo) + 15) / 16 * 16; }
+
+size_t plan_prep_smem(PrepArgs* a) {
+  const size_t wb = prep_win_bytes(a->n_obs), rb = (size_t)a->n_rt * sizeof(float);
+  a->win_in_smem = wb <= kPrepSmemBytes;
+  a->rt_in_smem = (a->win_in_smem ? wb : 0) + rb <= kPrepSmemBytes;
+  return (a->win_in_smem ? wb : 0) + (a->rt_in_smem ? rb : 0);
+}
 
 // Fragment m/z ordering key: NaN sorts after every number (ties by library
 // position), so the output positions always form a permutation.
@@ -248,13 +265,31 @@ __device__ int select_fragments(const PrepArgs& a, int64_t p, int lane, uint8_t*
 }
 
 __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a) {
+  extern __shared__ __align__(16) unsigned char prep_smem[];
   const int lane = threadIdx.x & 31;
+  const WinInfo* win = a.win;
+  const float* rt = a.rt;
+  {
+    size_t o = 0;
+    if (a.win_in_smem) {
+      WinInfo* ws = reinterpret_cast<WinInfo*>(prep_smem);
+      for (int i = threadIdx.x; i < a.n_obs; i += blockDim.x) ws[i] = a.win[i];
+      win = ws;
+      o = prep_win_bytes(a.n_obs);
+    }
+    if (a.rt_in_smem) {
+      float* rs = reinterpret_cast<float*>(prep_smem + o);
+      for (int i = threadIdx.x; i < a.n_rt; i += blockDim.x) rs[i] = __ldg(a.rt + i);
+      rt = rs;
+    }
+    __syncthreads();
+  }
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t p = warp0; p < a.n_prec; p += n_warps) {
     const float tol = a.ptol ? __ldg(a.ptol + p) : a.rt_tol;
     int cs, ce;
-    rt_limits(a.rt, a.n_rt, a.delta_t, __ldg(a.prt + p), tol, a.pad, &cs, &ce);
+    rt_limits(rt, a.n_rt, a.delta_t, __ldg(a.prt + p), tol, a.pad, &cs, &ce);
     bool skip = (ce - cs) < a.min_c;
     int nw = 0;
     if (!skip) {
@@ -263,7 +298,7 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a) {
         const int w = base + lane;
         bool hit = false;
         if (w < a.n_obs) {
-          const WinInfo wi = a.win[w];
+          const WinInfo wi = win[w];
           hit = wi.ss_off >= 0 && wi.lo <= pmz && wi.hi >= pmz;
         }
         const unsigned m = __ballot_sync(kFull, hit);
@@ -781,7 +816,8 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     ADS_CUDA(cudaEventRecord(s->stage_ev[0], st));
   }
   {
-    prep_kernel<<<(int)prep_blocks, kPrepThreads, 0, st>>>(pa);
+    const size_t prep_smem = plan_prep_smem(&pa);
+    prep_kernel<<<(int)prep_blocks, kPrepThreads, prep_smem, st>>>(pa);
     ADS_LAUNCH_CHECK();
     ++launches;
   }
@@ -1448,7 +1484,8 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   pa.blo = blo;
   pa.bhi = bhi;
   pa.err = flags;
-  prep_kernel<<<(int)prep_blocks, kPrepThreads, 0, st>>>(pa);
+  const size_t prep_smem = plan_prep_smem(&pa);
+  prep_kernel<<<(int)prep_blocks, kPrepThreads, prep_smem, st>>>(pa);
   ADS_LAUNCH_CHECK();
 
   int nw = kDefaultWarpsPerBlock;
