@@ -1,0 +1,44 @@
+"""Host-side helpers of bench.py that shape the reported line (no GPU needed)."""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+from alphadia_search_rs_b200 import synth  # noqa: E402
+
+
+def test_cpu_sample_windows_are_bounded_by_peaks():
+    # about 72 M peaks' worth of consecutive MS2 windows, whatever the run's shape
+    assert bench.sample_windows(synth.get_config("cfg1"), 0) == 24
+    assert bench.sample_windows(synth.get_config("cfg4"), 0) == 8
+    assert bench.sample_windows(synth.get_config("cfg0"), 0) == 8  # all of its windows
+    assert bench.sample_windows(synth.get_config("cfg1"), 5) == 5
+    assert bench.sample_windows(synth.get_config("cfg0"), 50) == 8
+
+
+def _rows(*rows):
+    keys = ("precursor_idx", "rank", "cycle_center", "score")
+    return {k: np.array([r[i] for r in rows]) for i, k in enumerate(keys)}
+
+
+def test_bf16_agreement_counts_matching_cycles_and_relative_errors():
+    ref = _rows((7, 0, 100, 10.0), (7, 1, 200, 5.0), (9, 0, 50, 2.0))
+    ref["score_f64"] = ref.pop("score").astype(np.float64)
+    got = _rows((7, 0, 100, 10.01), (7, 1, 201, 5.0), (9, 0, 50, 2.0))
+    agree, errs = bench.bf16_agreement(got, ref)
+    assert abs(agree - 2 / 3) < 1e-12
+    assert np.allclose(sorted(errs), [0.0, 0.001])
+
+
+def test_bf16_agreement_floors_the_denominator_near_zero():
+    # a score of 1e-9 next to the precursor's 10.0 is compared against 1e-3 * 10.0
+    ref = _rows((3, 0, 10, 10.0), (3, 1, 20, 1e-9))
+    ref["score_f64"] = ref.pop("score").astype(np.float64)
+    got = _rows((3, 0, 10, 10.0), (3, 1, 20, 1e-4))
+    agree, errs = bench.bf16_agreement(got, ref)
+    assert agree == 1.0
+    assert abs(max(errs) - (1e-4 - 1e-9) / 1e-2) < 1e-9
