@@ -1,16 +1,18 @@
 // PeakGroupSelection.search on the device (src/peak_group_selection/mod.rs:87-195).
 //
-// Three stages, all on one stream:
+// Stages, all on one stream:
 //   1. prep_kernel      one warp per precursor: RT cycle limits, quadrupole
 //                       windows, fragment filter / top-k / m/z sort, m/z bin
 //                       range of every kept fragment.
-//   2. search_kernel    one block per precursor (persistent blocks pulling from
-//                       an atomic counter): XIC gather into shared memory,
-//                       Gaussian convolution, log-dot score, 5-point local
-//                       maxima, top-K.  Arithmetic follows the reference's
-//                       operation order with explicitly rounded f32 ops, so the
-//                       only difference to the reference is its logf (see ln_rn).
-//   3. compaction       order-preserving concatenation of the per-precursor
+//   2. classify_kernel  precursors into RT-window length classes.
+//   3. search_kernel    one instance per class, one warp per precursor
+//                       (persistent warps pulling from an atomic counter): XIC
+//                       gather into shared memory, Gaussian convolution,
+//                       log-dot score, 5-point local maxima, top-K.  Arithmetic
+//                       follows the reference's operation order with explicitly
+//                       rounded f32 ops, so the only difference to the reference
+//                       is its logf (see ln_rn).
+//   4. compaction       order-preserving concatenation of the per-precursor
 //                       candidates into the nine to_arrays() columns.
 #include <algorithm>
 #include <array>
