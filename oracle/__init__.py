@@ -103,6 +103,31 @@ def lib():
                                         C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64),
                                         _f32p, _f32p, _f32p, _i64]),
         "orc_scores_f64_at": (C.c_double, [vp, vp, C.POINTER(OrcParams), _f32, _i64, _i64p, _i64, _f64p]),
+        # PeakGroupScoring
+        "orc_lib_set_scoring": (None, [vp, _u8p, _i64, _f32p]),
+        "orc_score": (vp, [vp, vp, _f32, _i64, _u64p, _u64p, _f32p, _u64p, _u64p, _u64p, _i64,
+                           C.c_int, C.c_int]),
+        "orc_features_len": (_i64, [vp]),
+        "orc_features_copy": (None, [vp, _u64p, _u64p, _f32p]),
+        "orc_features_free": (None, [vp]),
+        "orc_sc_normalize_profiles": (None, [_f32p, _i64, _i64, _i64, _f32p]),
+        "orc_sc_median_axis0": (None, [_f32p, _i64, _i64, C.c_int, _f32p]),
+        "orc_sc_correlation": (_f32, [_f32p, _f32p, _i64]),
+        "orc_sc_gamma_ln": (_f32, [_f32, C.c_int]),
+        "orc_sc_hyperscore": (_f32, [_u8p, _f32p, _u8p, vp, _i64, C.c_int]),
+        "orc_sc_longest_ion_series": (None, [_u8p, _u8p, _u8p, _i64, C.POINTER(C.c_uint8),
+                                              C.POINTER(C.c_uint8)]),
+        "orc_sc_intensity_ion_series": (_f32, [_u8p, _f32p, _u8p, _i64, C.c_uint8]),
+        "orc_sc_fwhm_rt": (_f32, [_f32p, _i64, _i64, _f32p]),
+        "orc_sc_fragment_mz_errors": (None, [_f32p, _f32p, _i64, _i64, _f32p, _f32p, _f32p]),
+        "orc_sc_weighted_mae": (_f32, [_f32p, _f32p, _i64]),
+        "orc_sc_median": (_f32, [_f32p, _i64]),
+        "orc_sc_std": (_f32, [_f32p, _i64]),
+        "orc_sc_ranked_mask": (None, [_f32p, _i64, _i64, _i64, _u8p]),
+        "orc_sc_count_above": (_i64, [_f32p, _i64, _f32, vp]),
+        "orc_sc_dot": (_f32, [_f32p, _f32p, _i64]),
+        "orc_sc_dense_xic_mz": (None, [vp, _f32, _i64, _i64, _f32, _f32p, _i64, _f32p, _f32p]),
+        "orc_sc_idf": (None, [vp, vp, _f32p, _i64, C.c_int, _f32p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -399,3 +424,187 @@ def scores_f64_at(dia: Dia, lb: Lib, params: Params, lib_pos, cycles, rt_toleran
     mx = lib().orc_scores_f64_at(dia._h, lb._h, C.byref(p), float(tol), int(lib_pos),
                                  cyc if len(cyc) else np.zeros(1, np.int64), len(cyc), out)
     return out[:len(cyc)], float(mx)
+
+
+# ------------------------------------------------------------ PeakGroupScoring
+
+# src/candidate/features.rs:6-48
+FEATURE_NAMES = (
+    "score", "mean_correlation", "median_correlation", "correlation_std", "intensity_correlation",
+    "num_fragments", "num_scans", "num_over_95", "num_over_90", "num_over_80", "num_over_50",
+    "num_over_0", "num_over_0_rank_0_5", "num_over_0_rank_6_11", "num_over_0_rank_12_17",
+    "num_over_0_rank_18_23", "num_over_50_rank_0_5", "num_over_50_rank_6_11",
+    "num_over_50_rank_12_17", "num_over_50_rank_18_23", "hyperscore_intensity_observation",
+    "hyperscore_intensity_library", "hyperscore_inverse_mass_error", "rt_observed", "delta_rt",
+    "longest_b_series", "longest_y_series", "naa", "weighted_mass_error", "log10_b_ion_intensity",
+    "log10_y_ion_intensity", "fwhm_rt", "idf_hyperscore", "idf_xic_dot_product",
+    "idf_intensity_dot_product", "median_profile_sum", "median_profile_sum_filtered",
+    "num_profiles", "num_profiles_filtered", "num_over_0_top6_idf", "num_over_50_top6_idf",
+)
+
+
+def lib_set_scoring(lb: "Lib", precursor_naa, fragment_mz_library) -> None:
+    """Adds SpecLibFlat's precursor_naa (input order) and fragment_mz_library."""
+    naa = np.ascontiguousarray(precursor_naa, np.uint8)
+    fml = _f32a(fragment_mz_library)
+    if len(fml) == 0:
+        fml = np.zeros(1, np.float32)
+        n = 0
+    else:
+        n = len(fml)
+    if len(naa) == 0:
+        naa = np.zeros(1, np.uint8)
+    lib().orc_lib_set_scoring(lb._h, naa, n, fml)
+
+
+def score(dia: "Dia", lb: "Lib", candidates: dict, mass_tolerance: float = 7.0,
+          top_k_fragments: int = 100, log_mode: int = LOG_GLIBC, n_threads: int = 0) -> dict:
+    """PeakGroupScoring.score (src/peak_group_scoring/mod.rs:42-101): a dict of
+    precursor_idx, rank and the 41 feature columns (src/candidate/features.rs:220-411)."""
+    L = lib()
+    n = len(candidates["precursor_idx"])
+    cols = [np.ascontiguousarray(candidates[k], np.uint64) for k in ("precursor_idx", "rank")]
+    sc = _f32a(candidates["score"])
+    cyc = [np.ascontiguousarray(candidates[k], np.uint64) for k in ("cycle_center", "cycle_start", "cycle_stop")]
+    if n == 0:
+        cols = [np.zeros(1, np.uint64)] * 2
+        sc = np.zeros(1, np.float32)
+        cyc = [np.zeros(1, np.uint64)] * 3
+    h = L.orc_score(dia._h, lb._h, float(mass_tolerance), int(top_k_fragments), cols[0], cols[1], sc,
+                    cyc[0], cyc[1], cyc[2], n, int(log_mode), int(n_threads or os.cpu_count() or 1))
+    try:
+        m = L.orc_features_len(h)
+        pidx = np.zeros(max(m, 1), np.uint64)
+        rank = np.zeros(max(m, 1), np.uint64)
+        feats = np.zeros((max(m, 1), len(FEATURE_NAMES)), np.float32)
+        L.orc_features_copy(h, pidx, rank, feats)
+    finally:
+        L.orc_features_free(h)
+    out = {"precursor_idx": pidx[:m], "rank": rank[:m]}
+    for k, name in enumerate(FEATURE_NAMES):
+        out[name] = np.ascontiguousarray(feats[:m, k])
+    return out
+
+
+def sc_normalize_profiles(x, dilations: int = 1) -> np.ndarray:
+    x = _f32a(np.atleast_2d(x))
+    out = np.zeros_like(x)
+    lib().orc_sc_normalize_profiles(x, x.shape[0], x.shape[1], dilations, out)
+    return out
+
+
+def sc_median_axis0(x, non_zero_only: bool = False) -> np.ndarray:
+    x = _f32a(x).reshape(-1, np.shape(x)[-1]) if np.size(x) else np.zeros((0, np.shape(x)[-1]), np.float32)
+    out = np.zeros(max(x.shape[1], 1), np.float32)
+    lib().orc_sc_median_axis0(x if x.size else np.zeros(1, np.float32), x.shape[0], x.shape[1],
+                              int(non_zero_only), out)
+    return out[:x.shape[1]]
+
+
+def _nz(a, dtype):
+    a = np.ascontiguousarray(a, dtype)
+    return a if a.size else np.zeros(1, dtype)
+
+
+def sc_correlation(x, y) -> float:
+    x, y = _f32a(x), _f32a(y)
+    if len(x) != len(y):
+        return 0.0
+    return float(lib().orc_sc_correlation(_nz(x, np.float32), _nz(y, np.float32), len(x)))
+
+
+def sc_gamma_ln(x: float, log_mode: int = LOG_GLIBC) -> float:
+    return float(lib().orc_sc_gamma_ln(float(x), int(log_mode)))
+
+
+def sc_hyperscore(types, intensities, mask, weights=None, log_mode: int = LOG_GLIBC) -> float:
+    n = len(types)
+    if len(intensities) != n or len(mask) != n or (weights is not None and len(weights) != n):
+        return 0.0  # src/peak_group_scoring/utils.rs:199-209
+    w = None if weights is None else _nz(weights, np.float32)
+    return float(lib().orc_sc_hyperscore(_nz(types, np.uint8), _nz(intensities, np.float32),
+                                         _nz(mask, np.uint8), w.ctypes.data if w is not None else None,
+                                         n, int(log_mode)))
+
+
+def sc_longest_ion_series(types, numbers, mask):
+    n = len(types)
+    if len(mask) != n or len(numbers) != n:
+        return (0, 0)  # src/peak_group_scoring/utils.rs:319-322
+    b, y = C.c_uint8(), C.c_uint8()
+    lib().orc_sc_longest_ion_series(_nz(types, np.uint8), _nz(numbers, np.uint8), _nz(mask, np.uint8), n,
+                                    C.byref(b), C.byref(y))
+    return (b.value, y.value)
+
+
+def sc_intensity_ion_series(types, intensities, mask, target: int) -> float:
+    n = len(types)
+    if len(intensities) != n or len(mask) != n:
+        return 0.0
+    return float(lib().orc_sc_intensity_ion_series(_nz(types, np.uint8), _nz(intensities, np.float32),
+                                                   _nz(mask, np.uint8), n, int(target)))
+
+
+def sc_fwhm_rt(profile, cycle_start: int, rt) -> float:
+    return float(lib().orc_sc_fwhm_rt(_nz(profile, np.float32), len(profile), int(cycle_start), _nz(rt, np.float32)))
+
+
+def sc_fragment_mz_errors(dense_mz, dense_xic, mz_library):
+    dm, dx = _f32a(np.atleast_2d(dense_mz)), _f32a(np.atleast_2d(dense_xic))
+    F, Cn = dm.shape
+    mo, err = np.zeros(max(F, 1), np.float32), np.zeros(max(F, 1), np.float32)
+    lib().orc_sc_fragment_mz_errors(_nz(dm, np.float32), _nz(dx, np.float32), F, Cn,
+                                    _nz(mz_library, np.float32), mo, err)
+    return mo[:F], err[:F]
+
+
+def sc_weighted_mae(errors, weights) -> float:
+    if len(errors) != len(weights):
+        return 0.0
+    return float(lib().orc_sc_weighted_mae(_nz(errors, np.float32), _nz(weights, np.float32), len(errors)))
+
+
+def sc_median(v) -> float:
+    return float(lib().orc_sc_median(_nz(v, np.float32), len(v)))
+
+
+def sc_std(v) -> float:
+    return float(lib().orc_sc_std(_nz(v, np.float32), len(v)))
+
+
+def sc_ranked_mask(v, r1: int, r2: int) -> np.ndarray:
+    out = np.zeros(max(len(v), 1), np.uint8)
+    lib().orc_sc_ranked_mask(_nz(v, np.float32), len(v), int(r1), int(r2), out)
+    return out[:len(v)].astype(bool)
+
+
+def sc_count_above(v, threshold: float, mask=None) -> int:
+    if mask is not None and len(mask) != len(v):
+        return 0
+    m = None if mask is None else _nz(mask, np.uint8)
+    return int(lib().orc_sc_count_above(_nz(v, np.float32), len(v), float(threshold),
+                                        m.ctypes.data if m is not None else None))
+
+
+def sc_dot(a, b) -> float:
+    if len(a) != len(b):
+        return 0.0
+    return float(lib().orc_sc_dot(_nz(a, np.float32), _nz(b, np.float32), len(a)))
+
+
+def sc_dense_xic_mz(dia: "Dia", precursor_mz: float, cycle_start: int, cycle_stop: int,
+                    mass_tolerance: float, fragment_mz):
+    fmz = _f32a(fragment_mz)
+    F, Cn = len(fmz), cycle_stop - cycle_start
+    xic = np.zeros(max(F * Cn, 1), np.float32)
+    mz = np.zeros(max(F * Cn, 1), np.float32)
+    lib().orc_sc_dense_xic_mz(dia._h, float(precursor_mz), int(cycle_start), int(cycle_stop),
+                              float(mass_tolerance), _nz(fmz, np.float32), F, xic, mz)
+    return xic[:F * Cn].reshape(F, Cn), mz[:F * Cn].reshape(F, Cn)
+
+
+def sc_idf(dia: "Dia", lb: "Lib", mz, log_mode: int = LOG_GLIBC) -> np.ndarray:
+    mz = _f32a(mz)
+    out = np.zeros(max(len(mz), 1), np.float32)
+    lib().orc_sc_idf(dia._h, lb._h, _nz(mz, np.float32), len(mz), int(log_mode), out)
+    return out[:len(mz)]

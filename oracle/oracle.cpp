@@ -26,6 +26,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -350,6 +351,10 @@ struct OrcLib {
   std::vector<uint64_t> frag_start, frag_stop;
   std::vector<float> fragment_mz, fragment_intensity;
   std::vector<uint8_t> fragment_number, fragment_type;
+  std::vector<int64_t> order;  // input position of each sorted precursor
+  // PeakGroupScoring inputs (orc_lib_set_scoring): naa in sorted order, library m/z
+  std::vector<uint8_t> precursor_naa;
+  std::vector<float> fragment_mz_library;
 };
 
 struct OrcCand {
@@ -581,6 +586,444 @@ void search_precursor(const OrcDia& d, const OrcLib& l, const OrcParams& p, floa
 
 // =================================================================== C API
 
+
+// ====================================================================
+// PeakGroupScoring.score (src/peak_group_scoring/mod.rs:42-340) and the
+// functions it calls.  Rust specifics restated:
+//   * `Iterator::sum` on f32 (Rust 1.88): a left fold that starts at -0.0
+//     (rust_sum); ndarray `sum_axis(Axis(1))` on a C-ordered matrix sums each
+//     contiguous row with ndarray's unrolled fold (ndarray_sum);
+//   * `sort_by(partial_cmp)` is stable (std::stable_sort); `powi(2)` is x * x;
+//   * `f32::ln`/`log10` are glibc logf/log10f (log_mode 0), or ln/log10 rounded
+//     once from double (log_mode 1, what the device computes);
+//   * u8 `a + 1` wraps (release build).
+// A correlation that comes out NaN or infinite makes the reference panic
+// (utils.rs:164-166); here it is 0.
+namespace {
+
+inline float log10_f32(float x, int mode) {
+  if (mode == 0) return log10f(x);
+  return (float)log10((double)x);
+}
+
+float rust_sum(const float* xs, int64_t n) {
+  float s = -0.0f;
+  for (int64_t i = 0; i < n; ++i) s = s + xs[i];
+  return s;
+}
+
+// src/quadrupole_observation/mod.rs:152-211
+void fill_xic_and_mz_slice(const OrcObs& o, const std::vector<float>& grid, float* xic, float* mzo,
+                           int64_t cs, int64_t ce, float tol, float mz) {
+  float delta = mz * tol * 1e-6f;
+  float lo = mz - delta;
+  float hi = mz + delta;
+  int64_t b0, b1;
+  mz_range_indices(grid.data(), (int64_t)grid.size(), lo, hi, &b0, &b1);
+  for (int64_t b = b0; b < b1; ++b) {
+    float actual = grid[(size_t)b];
+    int64_t s = o.slice_starts[(size_t)b];
+    int64_t e = o.slice_starts[(size_t)b + 1];
+    const uint16_t* cy = o.cycles.data() + s;
+    const float* in = o.intensities.data() + s;
+    int64_t pos = bsearch_u16(cy, e - s, (uint16_t)cs);
+    for (int64_t i = pos; i < e - s; ++i) {
+      int64_t c = cy[i];
+      if (c >= ce) break;
+      int64_t r = c - cs;
+      float v = in[i];
+      xic[r] = xic[r] + v;
+      if (v > 0.0f) {
+        float prev = xic[r] - v;
+        if (prev == 0.0f)
+          mzo[r] = actual;
+        else
+          mzo[r] = (mzo[r] * prev + actual * v) / xic[r];
+      }
+    }
+  }
+}
+
+// src/dense_xic_observation/mod.rs:97-137
+void dense_xic_mz(const OrcDia& d, float pmz, int64_t cs, int64_t ce, float tol, const float* fmz,
+                  int64_t F, float* xic, float* mzo) {
+  int64_t C = ce - cs;
+  std::fill(xic, xic + F * C, 0.0f);
+  std::fill(mzo, mzo + F * C, 0.0f);
+  std::vector<int64_t> win;
+  valid_observations(d, pmz, win);
+  for (auto w : win)
+    for (int64_t f = 0; f < F; ++f)
+      fill_xic_and_mz_slice(d.obs[(size_t)w], d.grid, xic + f * C, mzo + f * C, cs, ce, tol, fmz[f]);
+}
+
+// src/peak_group_scoring/utils.rs:71-109
+void normalize_profiles(const float* x, int64_t R, int64_t C, int64_t dil, float* out) {
+  int64_t center = C / 2;
+  int64_t a = center > dil ? center - dil : 0;
+  int64_t b = std::min(center + dil + 1, C);
+  for (int64_t i = 0; i < R; ++i) {
+    float sum = 0.0f;
+    int64_t count = 0;
+    for (int64_t j = a; j < b; ++j) {
+      sum = sum + x[i * C + j];
+      ++count;
+    }
+    float mean = count > 0 ? sum / (float)count : 0.0f;
+    for (int64_t j = 0; j < C; ++j) out[i * C + j] = mean > 0.0f ? x[i * C + j] / mean : 0.0f;
+  }
+}
+
+// src/peak_group_scoring/utils.rs:7-29 (rows with a non-zero value, in order)
+std::vector<int64_t> non_zero_rows(const float* x, int64_t R, int64_t C) {
+  std::vector<int64_t> rows;
+  for (int64_t i = 0; i < R; ++i)
+    for (int64_t j = 0; j < C; ++j)
+      if (x[i * C + j] != 0.0f) {
+        rows.push_back(i);
+        break;
+      }
+  return rows;
+}
+
+bool partial_less(float a, float b) { return a < b; }  // NaN compares Equal
+
+// src/peak_group_scoring/utils.rs:35-66 over the given rows
+void median_axis_0(const float* x, const std::vector<int64_t>& rows, int64_t C, float* out) {
+  const int64_t R = (int64_t)rows.size();
+  std::vector<float> col((size_t)R);
+  for (int64_t j = 0; j < C; ++j) {
+    if (R == 0) {
+      out[j] = 0.0f;
+      continue;
+    }
+    for (int64_t i = 0; i < R; ++i) col[(size_t)i] = x[rows[(size_t)i] * C + j];
+    std::stable_sort(col.begin(), col.end(), partial_less);
+    out[j] = R % 2 == 0 ? (col[(size_t)(R / 2 - 1)] + col[(size_t)(R / 2)]) / 2.0f : col[(size_t)(R / 2)];
+  }
+}
+
+// src/peak_group_scoring/utils.rs:126-172
+float correlation_safe(const float* x, const float* y, int64_t n) {
+  if (n == 0) return 0.0f;
+  float xs = rust_sum(x, n), ys = rust_sum(y, n);
+  if (xs == 0.0f || ys == 0.0f) return 0.0f;
+  float xm = xs / (float)n, ym = ys / (float)n;
+  float xv = 0.0f, yv = 0.0f, cv = 0.0f;
+  for (int64_t i = 0; i < n; ++i) {
+    float dx = x[i] - xm, dy = y[i] - ym;
+    xv = xv + dx * dx;
+    yv = yv + dy * dy;
+    cv = cv + dx * dy;
+  }
+  if (xv == 0.0f || yv == 0.0f) return 0.0f;
+  float c = cv / (sqrtf(xv) * sqrtf(yv));
+  if (std::isnan(c) || std::isinf(c)) return 0.0f;
+  return std::min(std::max(c, -1.0f), 1.0f);
+}
+
+// src/peak_group_scoring/utils.rs:293-312
+float gamma_ln(float x, int mode) {
+  if (x <= 0.0f) return 0.0f;
+  if (fabsf(x - 1.0f) < 1e-6f) return 0.0f;
+  if (fabsf(x - 2.0f) < 1e-6f) return 0.0f;
+  const float ln_2pi = 1.837877f;
+  return (x - 0.5f) * log_f32(x, mode) - x + 0.5f * ln_2pi;
+}
+
+// src/peak_group_scoring/utils.rs:193-279 (weights null: 1.0)
+float hyperscore_weighted(const uint8_t* type, const float* inten, const bool* mask,
+                          const float* w, int64_t n, int mode) {
+  uint32_t nb = 0, ny = 0;
+  float sb = 0.0f, sy = 0.0f;
+  for (int64_t i = 0; i < n; ++i) {
+    if (!mask[i] || inten[i] == 0.0f) continue;
+    float wi = inten[i] * (w ? w[i] : 1.0f);
+    if (type[i] == 98) {
+      ++nb;
+      sb = sb + wi;
+    } else if (type[i] == 121) {
+      ++ny;
+      sy = sy + wi;
+    }
+  }
+  if (nb == 0 && ny == 0) return 0.0f;
+  float fb = nb > 0 ? gamma_ln((float)nb + 1.0f, mode) : 0.0f;
+  float fy = ny > 0 ? gamma_ln((float)ny + 1.0f, mode) : 0.0f;
+  float lb = sb > 0.0f ? log_f32(sb, mode) : 0.0f;
+  float ly = sy > 0.0f ? log_f32(sy, mode) : 0.0f;
+  float h = fb + fy + lb + ly;
+  return std::isfinite(h) ? h : 0.0f;
+}
+
+// src/peak_group_scoring/utils.rs:314-372
+void longest_ion_series(const uint8_t* type, const uint8_t* number, const bool* mask, int64_t n,
+                        uint8_t* lb, uint8_t* ly) {
+  std::vector<uint8_t> b, y;
+  for (int64_t i = 0; i < n; ++i) {
+    if (!mask[i]) continue;
+    if (type[i] == 98) b.push_back(number[i]);
+    if (type[i] == 121) y.push_back(number[i]);
+  }
+  auto longest = [](std::vector<uint8_t> v) -> uint8_t {
+    if (v.empty()) return 0;
+    std::sort(v.begin(), v.end());
+    uint8_t mx = 1, cur = 1;
+    for (size_t i = 1; i < v.size(); ++i) {
+      if (v[i] == (uint8_t)(v[i - 1] + 1)) {
+        cur = (uint8_t)(cur + 1);
+        mx = std::max(mx, cur);
+      } else {
+        cur = 1;
+      }
+    }
+    return mx;
+  };
+  *lb = longest(b);
+  *ly = longest(y);
+}
+
+// src/peak_group_scoring/utils.rs:402-429
+float intensity_ion_series(const uint8_t* type, const float* inten, const bool* mask, int64_t n,
+                           uint8_t target) {
+  float t = 0.0f;
+  for (int64_t i = 0; i < n; ++i)
+    if (mask[i] && inten[i] > 0.0f && type[i] == target) t = t + inten[i];
+  return t;
+}
+
+// src/peak_group_scoring/utils.rs:431-437
+float dot_product(const float* a, const float* b, int64_t n) {
+  if (n == 0) return 0.0f;
+  float s = -0.0f;
+  for (int64_t i = 0; i < n; ++i) s = s + a[i] * b[i];
+  return s;
+}
+
+// src/peak_group_scoring/utils.rs:453-476
+float fwhm_rt(const float* prof, int64_t C, int64_t cs, const float* rt) {
+  if (C == 0) return 0.0f;
+  int64_t half = C / 2;
+  float center = prof[half];
+  for (int64_t i = 0; i < half; ++i) {
+    float mean = (prof[half - i] + prof[half + i]) / 2.0f;
+    if (mean <= center / 2.0f) return rt[cs + half + i] - rt[cs + half - i];
+  }
+  return 0.0f;
+}
+
+// src/utils/mod.rs:41-75 and :11-39
+void fragment_mz_errors(const float* dmz, const float* dxic, int64_t F, int64_t C,
+                        const float* mz_lib, float* mz_obs, float* err) {
+  for (int64_t f = 0; f < F; ++f) {
+    float ws = 0.0f, wsum = 0.0f;
+    for (int64_t j = 0; j < C; ++j) {
+      float w = dxic[f * C + j];
+      if (w > 0.0f) {
+        ws = ws + dmz[f * C + j] * w;
+        wsum = wsum + w;
+      }
+    }
+    float o = wsum > 0.0f ? ws / wsum : 0.0f;
+    mz_obs[f] = o;
+    err[f] = o > 0.0f ? ((o - mz_lib[f]) / mz_lib[f]) * 1e6f : 0.0f;
+  }
+}
+
+// src/utils/mod.rs:83-117
+float weighted_mean_abs_error(const float* err, const float* w, int64_t n) {
+  if (n == 0) return 0.0f;
+  float ws = 0.0f, wsum = 0.0f;
+  for (int64_t i = 0; i < n; ++i)
+    if (w[i] > 0.0f && err[i] != 0.0f) {
+      ws = ws + fabsf(err[i]) * w[i];
+      wsum = wsum + w[i];
+    }
+  return wsum > 0.0f ? ws / wsum : 0.0f;
+}
+
+// src/utils/mod.rs:120-143
+float median_of(const float* v, int64_t n) {
+  if (n == 0) return 0.0f;
+  std::vector<float> s(v, v + n);
+  std::stable_sort(s.begin(), s.end(), partial_less);
+  int64_t mid = n / 2;
+  return n % 2 == 0 ? (s[(size_t)(mid - 1)] + s[(size_t)mid]) / 2.0f : s[(size_t)mid];
+}
+
+// src/utils/mod.rs:146-173
+float std_of(const float* v, int64_t n) {
+  if (n < 2) return 0.0f;
+  float mean = rust_sum(v, n) / (float)n;
+  float acc = -0.0f;
+  for (int64_t i = 0; i < n; ++i) acc = acc + (v[i] - mean) * (v[i] - mean);
+  return sqrtf(acc / (float)(n - 1));
+}
+
+// src/utils/mod.rs:175-221
+void ranked_mask(const float* v, int64_t n, int64_t r1, int64_t r2, bool* out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = false;
+  if (n == 0 || r1 >= r2) return;
+  std::vector<int64_t> idx((size_t)n);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+    if (v[b] < v[a]) return true;   // value descending
+    if (v[a] < v[b]) return false;
+    return a < b;                   // then index ascending (NaN compares Equal)
+  });
+  for (int64_t r = std::min(r1, n); r < std::min(r2, n); ++r) out[idx[(size_t)r]] = true;
+}
+
+// src/utils/mod.rs:223-237
+int64_t count_above(const float* v, int64_t n, float thr, const bool* mask) {
+  int64_t c = 0;
+  for (int64_t i = 0; i < n; ++i)
+    if ((!mask || mask[i]) && v[i] > thr) ++c;
+  return c;
+}
+
+constexpr int kNumFeatures = 41;
+
+struct OrcFeatureRow {
+  uint64_t precursor_idx, rank;
+  float f[kNumFeatures];
+};
+
+struct Idf {
+  std::vector<uint32_t> counts;
+  float total = 0.0f;
+};
+
+// src/idf/mod.rs:13-33 over the library's fragment_mz_library
+Idf build_idf(const OrcDia& d, const OrcLib& l) {
+  Idf idf;
+  idf.counts.assign(d.grid.size(), 0u);
+  idf.total = (float)l.fragment_mz_library.size();
+  for (float mz : l.fragment_mz_library)
+    ++idf.counts[(size_t)find_closest_index(d.grid.data(), (int64_t)d.grid.size(), mz)];
+  return idf;
+}
+
+// src/idf/mod.rs:35-48
+float idf_of(const Idf& idf, const OrcDia& d, float mz, int mode) {
+  if (idf.total == 0.0f) return 1.0f;
+  uint32_t c = idf.counts[(size_t)find_closest_index(d.grid.data(), (int64_t)d.grid.size(), mz)];
+  return log_f32(idf.total / (float)std::max(c, 1u), mode);
+}
+
+// src/peak_group_scoring/mod.rs:104-340 for one candidate whose precursor sits at
+// sorted position i.
+void score_candidate(const OrcDia& d, const OrcLib& l, const Idf& idf, float tol, int64_t top_k,
+                     int64_t i, uint64_t pidx, uint64_t rank, float cand_score, uint64_t center,
+                     uint64_t cstart, uint64_t cstop, int mode, OrcFeatureRow& out) {
+  // get_precursor_by_idx_filtered(idx, non_zero = true, y1 = true, top_k)
+  const int64_t s = (int64_t)l.frag_start[(size_t)i], e = (int64_t)l.frag_stop[(size_t)i];
+  auto keep = filter_sort_fragments(e - s, l.fragment_mz.data() + s, l.fragment_intensity.data() + s,
+                                    l.fragment_number.data() + s, l.fragment_type.data() + s,
+                                    true, true, top_k);
+  const int64_t F = (int64_t)keep.size();
+  std::vector<float> fmz, fmzl, fint;
+  std::vector<uint8_t> ftype, fnum;
+  for (auto k : keep) {
+    fmz.push_back(l.fragment_mz[(size_t)(s + k)]);
+    fmzl.push_back(l.fragment_mz_library[(size_t)(s + k)]);
+    fint.push_back(l.fragment_intensity[(size_t)(s + k)]);
+    ftype.push_back(l.fragment_type[(size_t)(s + k)]);
+    fnum.push_back(l.fragment_number[(size_t)(s + k)]);
+  }
+  const int64_t cs = (int64_t)cstart, C = (int64_t)cstop - (int64_t)cstart;
+  std::vector<float> xic((size_t)(F * C)), mzo((size_t)(F * C)), norm((size_t)(F * C));
+  dense_xic_mz(d, l.precursor_mz[(size_t)i], cs, (int64_t)cstop, tol, fmz.data(), F, xic.data(),
+               mzo.data());
+  normalize_profiles(xic.data(), F, C, 1, norm.data());
+  std::vector<int64_t> all((size_t)F);
+  std::iota(all.begin(), all.end(), 0);
+  auto nz = non_zero_rows(norm.data(), F, C);
+  std::vector<float> med((size_t)C), med_f((size_t)C);
+  median_axis_0(norm.data(), all, C, med.data());
+  median_axis_0(norm.data(), nz, C, med_f.data());
+  const float med_sum = rust_sum(med.data(), C), med_sum_f = rust_sum(med_f.data(), C);
+  const float fwhm = fwhm_rt(med_f.data(), C, cs, d.rt.data());
+  std::vector<float> corr((size_t)F);
+  for (int64_t f = 0; f < F; ++f) corr[(size_t)f] = correlation_safe(med_f.data(), norm.data() + f * C, C);
+  std::vector<float> obs((size_t)F);
+  for (int64_t f = 0; f < F; ++f) obs[(size_t)f] = ndarray_sum(xic.data() + f * C, C);
+  const float int_corr = correlation_safe(obs.data(), fint.data(), F);
+  const float mean_corr = F > 0 ? rust_sum(corr.data(), F) / (float)F : 0.0f;
+  const float med_corr = median_of(corr.data(), F);
+  const float std_corr = std_of(corr.data(), F);
+  std::unique_ptr<bool[]> m0(new bool[(size_t)F + 1]), m1(new bool[(size_t)F + 1]),
+      m2(new bool[(size_t)F + 1]), m3(new bool[(size_t)F + 1]), matched(new bool[(size_t)F + 1]),
+      m6(new bool[(size_t)F + 1]);
+  ranked_mask(fint.data(), F, 0, 6, m0.get());
+  ranked_mask(fint.data(), F, 6, 12, m1.get());
+  ranked_mask(fint.data(), F, 12, 18, m2.get());
+  ranked_mask(fint.data(), F, 18, 24, m3.get());
+  for (int64_t f = 0; f < F; ++f) matched[(size_t)f] = obs[(size_t)f] > 0.0f;
+  std::vector<float> mz_obs((size_t)F), err((size_t)F), inv_w((size_t)F), idf_v((size_t)F);
+  fragment_mz_errors(mzo.data(), xic.data(), F, C, fmz.data(), mz_obs.data(), err.data());
+  for (int64_t f = 0; f < F; ++f) inv_w[(size_t)f] = 1.0f / (fabsf(err[(size_t)f]) + 0.1f);
+  for (int64_t f = 0; f < F; ++f) idf_v[(size_t)f] = idf_of(idf, d, fmzl[(size_t)f], mode);
+  ranked_mask(idf_v.data(), F, 0, 6, m6.get());
+  const float rt_obs = d.rt[(size_t)center];
+  const float ib = intensity_ion_series(ftype.data(), obs.data(), matched.get(), F, 98);
+  const float iy = intensity_ion_series(ftype.data(), obs.data(), matched.get(), F, 121);
+  const float idf_int_dot = dot_product(idf_v.data(), obs.data(), F);
+  uint8_t lb = 0, ly = 0;
+  longest_ion_series(ftype.data(), fnum.data(), matched.get(), F, &lb, &ly);
+  const float* c = corr.data();
+  float* o = out.f;
+  out.precursor_idx = pidx;
+  out.rank = rank;
+  o[0] = cand_score;
+  o[1] = mean_corr;
+  o[2] = med_corr;
+  o[3] = std_corr;
+  o[4] = int_corr;
+  o[5] = (float)F;
+  o[6] = (float)(uint64_t)C;
+  o[7] = (float)count_above(c, F, 0.95f, nullptr);
+  o[8] = (float)count_above(c, F, 0.90f, nullptr);
+  o[9] = (float)count_above(c, F, 0.80f, nullptr);
+  o[10] = (float)count_above(c, F, 0.50f, nullptr);
+  o[11] = (float)count_above(c, F, 0.0f, nullptr);
+  o[12] = (float)count_above(c, F, 0.0f, m0.get());
+  o[13] = (float)count_above(c, F, 0.0f, m1.get());
+  o[14] = (float)count_above(c, F, 0.0f, m2.get());
+  o[15] = (float)count_above(c, F, 0.0f, m3.get());
+  o[16] = (float)count_above(c, F, 0.50f, m0.get());
+  o[17] = (float)count_above(c, F, 0.50f, m1.get());
+  o[18] = (float)count_above(c, F, 0.50f, m2.get());
+  o[19] = (float)count_above(c, F, 0.50f, m3.get());
+  o[20] = hyperscore_weighted(ftype.data(), obs.data(), matched.get(), nullptr, F, mode);
+  o[21] = hyperscore_weighted(ftype.data(), fint.data(), matched.get(), nullptr, F, mode);
+  o[22] = hyperscore_weighted(ftype.data(), obs.data(), matched.get(), inv_w.data(), F, mode);
+  o[23] = rt_obs;
+  o[24] = rt_obs - l.precursor_rt[(size_t)i];
+  o[25] = (float)lb;
+  o[26] = (float)ly;
+  o[27] = (float)l.precursor_naa[(size_t)i];
+  o[28] = weighted_mean_abs_error(err.data(), fint.data(), F);
+  o[29] = log10_f32(ib + 1e-8f, mode);
+  o[30] = log10_f32(iy + 1e-8f, mode);
+  o[31] = fwhm;
+  o[32] = hyperscore_weighted(ftype.data(), idf_v.data(), matched.get(), nullptr, F, mode);
+  o[33] = dot_product(idf_v.data(), c, F);
+  o[34] = log10_f32(idf_int_dot + 1e-8f, mode);
+  o[35] = med_sum;
+  o[36] = med_sum_f;
+  o[37] = (float)F;
+  o[38] = (float)nz.size();
+  o[39] = (float)count_above(c, F, 0.0f, m6.get());
+  o[40] = (float)count_above(c, F, 0.50f, m6.get());
+}
+
+}  // namespace
+
+struct OrcFeatures {
+  std::vector<OrcFeatureRow> rows;
+};
+
 extern "C" {
 
 int64_t orc_ppm_index_len(float r, float s, float e) { return (int64_t)ppm_index(r, s, e).size(); }
@@ -718,6 +1161,7 @@ OrcLib* orc_lib_build(int64_t P, const uint64_t* pidx, const float* pmz, const f
   std::vector<int64_t> ord((size_t)P);
   std::iota(ord.begin(), ord.end(), 0);
   std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) { return pidx[a] < pidx[b]; });
+  l->order = ord;
   for (auto i : ord) {
     l->precursor_idx.push_back(pidx[i]);
     l->precursor_mz.push_back(pmz[i]);
@@ -815,6 +1259,123 @@ double orc_scores_f64_at(const OrcDia* d, const OrcLib* l, const OrcParams* p, f
     out[q] = (j >= 0 && j < C) ? score[(size_t)j] : 0.0;
   }
   return mx;
+}
+
+
+// ---- PeakGroupScoring (src/peak_group_scoring/mod.rs:42-340)
+
+void orc_lib_set_scoring(OrcLib* l, const uint8_t* naa, int64_t n_frag, const float* fmz_library) {
+  // SpecLibFlat::from_arrays (src/speclib_flat/mod.rs:100-188): precursor_naa follows the
+  // stable precursor sort, fragment_mz_library keeps the input order
+  l->precursor_naa.clear();
+  for (auto i : l->order) l->precursor_naa.push_back(naa ? naa[i] : 0);
+  l->fragment_mz_library.assign(fmz_library, fmz_library + n_frag);
+}
+
+OrcFeatures* orc_score(const OrcDia* d, const OrcLib* l, float mass_tolerance, int64_t top_k,
+                       const uint64_t* pidx, const uint64_t* rank, const float* score,
+                       const uint64_t* center, const uint64_t* start, const uint64_t* stop,
+                       int64_t n, int log_mode, int n_threads) {
+  Idf idf = build_idf(*d, *l);
+  std::vector<OrcFeatureRow> rows((size_t)n);
+  std::vector<char> found((size_t)n, 0);
+  const int64_t P = (int64_t)l->precursor_idx.size();
+  const uint64_t* keys = l->precursor_idx.data();
+  parallel_for(n, n_threads, 64, [&](int64_t q) {
+    // SpecLibFlat::get_precursor_by_idx_filtered: binary_search on the sorted idx
+    const uint64_t x = pidx[q];
+    int64_t i = rust_bsearch(
+        P, [&](int64_t m) { return keys[m] > x; }, [&](int64_t m) { return keys[m] == x; },
+        [&](int64_t m) { return keys[m] < x; });
+    if (i >= P || keys[i] != x) return;  // skipped with a warning in the reference
+    score_candidate(*d, *l, idf, mass_tolerance, top_k, i, x, rank[q], score[q], center[q],
+                    start[q], stop[q], log_mode, rows[(size_t)q]);
+    found[(size_t)q] = 1;
+  });
+  auto* r = new OrcFeatures();
+  for (int64_t q = 0; q < n; ++q)
+    if (found[(size_t)q]) r->rows.push_back(rows[(size_t)q]);
+  return r;
+}
+
+int64_t orc_features_len(const OrcFeatures* r) { return (int64_t)r->rows.size(); }
+
+void orc_features_copy(const OrcFeatures* r, uint64_t* pidx, uint64_t* rank, float* feats) {
+  for (size_t q = 0; q < r->rows.size(); ++q) {
+    pidx[q] = r->rows[q].precursor_idx;
+    rank[q] = r->rows[q].rank;
+    for (int k = 0; k < kNumFeatures; ++k) feats[q * kNumFeatures + k] = r->rows[q].f[k];
+  }
+}
+
+void orc_features_free(OrcFeatures* r) { delete r; }
+
+// ---- the scoring helpers on raw arrays (for the reference's unit-test values)
+
+void orc_sc_normalize_profiles(const float* x, int64_t R, int64_t C, int64_t dil, float* out) {
+  normalize_profiles(x, R, C, dil, out);
+}
+void orc_sc_median_axis0(const float* x, int64_t R, int64_t C, int non_zero_only, float* out) {
+  std::vector<int64_t> rows;
+  if (non_zero_only) {
+    rows = non_zero_rows(x, R, C);
+  } else {
+    rows.resize((size_t)R);
+    std::iota(rows.begin(), rows.end(), 0);
+  }
+  median_axis_0(x, rows, C, out);
+}
+float orc_sc_correlation(const float* x, const float* y, int64_t n) { return correlation_safe(x, y, n); }
+float orc_sc_gamma_ln(float x, int mode) { return gamma_ln(x, mode); }
+float orc_sc_hyperscore(const uint8_t* type, const float* inten, const uint8_t* mask,
+                        const float* w, int64_t n, int mode) {
+  std::unique_ptr<bool[]> m(new bool[(size_t)n + 1]);
+  for (int64_t i = 0; i < n; ++i) m[(size_t)i] = mask[i] != 0;
+  return hyperscore_weighted(type, inten, m.get(), w, n, mode);
+}
+void orc_sc_longest_ion_series(const uint8_t* type, const uint8_t* number, const uint8_t* mask,
+                               int64_t n, uint8_t* lb, uint8_t* ly) {
+  std::unique_ptr<bool[]> m(new bool[(size_t)n + 1]);
+  for (int64_t i = 0; i < n; ++i) m[(size_t)i] = mask[i] != 0;
+  longest_ion_series(type, number, m.get(), n, lb, ly);
+}
+float orc_sc_intensity_ion_series(const uint8_t* type, const float* inten, const uint8_t* mask,
+                                  int64_t n, uint8_t target) {
+  std::unique_ptr<bool[]> m(new bool[(size_t)n + 1]);
+  for (int64_t i = 0; i < n; ++i) m[(size_t)i] = mask[i] != 0;
+  return intensity_ion_series(type, inten, m.get(), n, target);
+}
+float orc_sc_fwhm_rt(const float* prof, int64_t C, int64_t cs, const float* rt) {
+  return fwhm_rt(prof, C, cs, rt);
+}
+void orc_sc_fragment_mz_errors(const float* dmz, const float* dxic, int64_t F, int64_t C,
+                               const float* mz_lib, float* mz_obs, float* err) {
+  fragment_mz_errors(dmz, dxic, F, C, mz_lib, mz_obs, err);
+}
+float orc_sc_weighted_mae(const float* err, const float* w, int64_t n) {
+  return weighted_mean_abs_error(err, w, n);
+}
+float orc_sc_median(const float* v, int64_t n) { return median_of(v, n); }
+float orc_sc_std(const float* v, int64_t n) { return std_of(v, n); }
+void orc_sc_ranked_mask(const float* v, int64_t n, int64_t r1, int64_t r2, uint8_t* out) {
+  std::unique_ptr<bool[]> m(new bool[(size_t)n + 1]);
+  ranked_mask(v, n, r1, r2, m.get());
+  for (int64_t i = 0; i < n; ++i) out[i] = m[(size_t)i] ? 1 : 0;
+}
+int64_t orc_sc_count_above(const float* v, int64_t n, float thr, const uint8_t* mask) {
+  if (!mask) return count_above(v, n, thr, nullptr);
+  std::unique_ptr<bool[]> m(new bool[(size_t)n + 1]);
+  for (int64_t i = 0; i < n; ++i) m[(size_t)i] = mask[i] != 0;
+  return count_above(v, n, thr, m.get());
+}
+float orc_sc_dot(const float* a, const float* b, int64_t n) { return dot_product(a, b, n); }
+void orc_sc_dense_xic_mz(const OrcDia* d, float pmz, int64_t cs, int64_t ce, float tol,
+                         const float* fmz, int64_t F, float* xic, float* mzo) {
+  dense_xic_mz(*d, pmz, cs, ce, tol, fmz, F, xic, mzo);
+}
+void orc_sc_idf(const OrcDia* d, const OrcLib* l, const float* mz, int64_t n, int mode, float* out) {
+  Idf idf = build_idf(*d, *l);
+  for (int64_t i = 0; i < n; ++i) out[i] = idf_of(idf, *d, mz[i], mode);
 }
 
 }  // extern "C"

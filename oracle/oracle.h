@@ -146,6 +146,47 @@ double orc_scores_f64_at(const OrcDia* d, const OrcLib* l, const OrcParams* p,
                          float rt_tolerance, int64_t lib_pos, const int64_t* cycles, int64_t n,
                          double* out);
 
+
+/* ---- PeakGroupScoring: src/peak_group_scoring/mod.rs:42-340 ---- */
+typedef struct OrcFeatures OrcFeatures;
+/* precursor_naa in input order; fragment_mz_library (n_frag, input order) */
+void orc_lib_set_scoring(OrcLib* l, const uint8_t* precursor_naa, int64_t n_frag,
+                         const float* fragment_mz_library);
+/* Candidates in the order given; those whose precursor_idx is not in the library are
+ * skipped.  41 features per row in FEATURE_NAMES order (src/candidate/features.rs:6-48). */
+OrcFeatures* orc_score(const OrcDia* d, const OrcLib* l, float mass_tolerance, int64_t top_k,
+                       const uint64_t* precursor_idx, const uint64_t* rank, const float* score,
+                       const uint64_t* cycle_center, const uint64_t* cycle_start,
+                       const uint64_t* cycle_stop, int64_t n, int log_mode, int n_threads);
+int64_t orc_features_len(const OrcFeatures* r);
+void orc_features_copy(const OrcFeatures* r, uint64_t* precursor_idx, uint64_t* rank, float* feats);
+void orc_features_free(OrcFeatures* r);
+/* the scoring helpers, for the reference's unit-test values */
+void orc_sc_normalize_profiles(const float* x, int64_t rows, int64_t cols, int64_t dil, float* out);
+void orc_sc_median_axis0(const float* x, int64_t rows, int64_t cols, int non_zero_only, float* out);
+float orc_sc_correlation(const float* x, const float* y, int64_t n);
+float orc_sc_gamma_ln(float x, int log_mode);
+float orc_sc_hyperscore(const uint8_t* type, const float* inten, const uint8_t* mask,
+                        const float* weights, int64_t n, int log_mode);
+void orc_sc_longest_ion_series(const uint8_t* type, const uint8_t* number, const uint8_t* mask,
+                               int64_t n, uint8_t* longest_b, uint8_t* longest_y);
+float orc_sc_intensity_ion_series(const uint8_t* type, const float* inten, const uint8_t* mask,
+                                  int64_t n, uint8_t target);
+float orc_sc_fwhm_rt(const float* profile, int64_t n, int64_t cycle_start, const float* rt);
+void orc_sc_fragment_mz_errors(const float* dense_mz, const float* dense_xic, int64_t F, int64_t C,
+                               const float* mz_library, float* mz_observed, float* mass_error);
+float orc_sc_weighted_mae(const float* err, const float* weights, int64_t n);
+float orc_sc_median(const float* v, int64_t n);
+float orc_sc_std(const float* v, int64_t n);
+void orc_sc_ranked_mask(const float* v, int64_t n, int64_t r1, int64_t r2, uint8_t* out);
+int64_t orc_sc_count_above(const float* v, int64_t n, float threshold, const uint8_t* mask);
+float orc_sc_dot(const float* a, const float* b, int64_t n);
+void orc_sc_dense_xic_mz(const OrcDia* d, float precursor_mz, int64_t cycle_start,
+                         int64_t cycle_stop, float mass_tolerance, const float* fragment_mz,
+                         int64_t F, float* xic, float* mz);
+void orc_sc_idf(const OrcDia* d, const OrcLib* l, const float* mz, int64_t n, int log_mode,
+                float* out);
+
 #ifdef __cplusplus
 }
 #endif
