@@ -86,6 +86,13 @@ class AdsSelectionParams(C.Structure):
     ]
 
 
+class AdsScoringParams(C.Structure):
+    _fields_ = [
+        ("mass_tolerance", f32),
+        ("top_k_fragments", i64),
+    ]
+
+
 class AdsEngineOptions(C.Structure):
     _fields_ = [
         ("precision", i32),
@@ -144,6 +151,14 @@ SIGNATURES = {
     "ads_candidates_size": (i64, [vp]),
     "ads_candidates_copy_out": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "ads_candidates_destroy": (C.c_int, [vp]),
+    "ads_scoring_params_default": (None, [C.POINTER(AdsScoringParams)]),
+    "ads_score": (C.c_int, [C.POINTER(AdsScoringParams), vp, vp, vp, C.c_int, C.POINTER(vp)]),
+    "ads_score_arrays": (C.c_int, [C.POINTER(AdsScoringParams), vp, vp, i64, vp, vp, vp, vp, vp, vp,
+                                   C.c_int, C.c_int, C.POINTER(vp)]),
+    "ads_features_size": (i64, [vp]),
+    "ads_features_copy_out": (C.c_int, [vp, vp, vp, vp]),
+    "ads_features_destroy": (C.c_int, [vp]),
+    "ads_feature_names": (C.c_int, [C.POINTER(C.c_char_p), C.c_int]),
 }
 
 _lib = None

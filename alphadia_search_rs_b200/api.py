@@ -584,3 +584,146 @@ def mz_grid() -> np.ndarray:
 
 def device_count() -> int:
     return int(_lib().ads_device_count())
+
+
+# ------------------------------------------------------------------ scoring
+
+class ScoringParameters:
+    """ScoringParameters (src/peak_group_scoring/parameters.rs:4-40): read-only
+    mass_tolerance and top_k_fragments, defaults of ``new``, and ``update(dict)``."""
+
+    __slots__ = ("_v",)
+
+    def __init__(self):
+        p = F.AdsScoringParams()
+        _lib().ads_scoring_params_default(C.byref(p))
+        object.__setattr__(self, "_v", {"mass_tolerance": float(np.float32(p.mass_tolerance)),
+                                        "top_k_fragments": int(p.top_k_fragments)})
+
+    def __getattr__(self, name):
+        v = object.__getattribute__(self, "_v")
+        if name in v:
+            return v[name]
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        raise AttributeError(f"attribute '{name}' of 'ScoringParameters' objects is not writable")
+
+    def update(self, config: dict) -> None:
+        """Sets mass_tolerance and/or top_k_fragments (parameters.rs:28-37)."""
+        new = dict(self._v)
+        if "mass_tolerance" in config:
+            val = config["mass_tolerance"]
+            if isinstance(val, (bool, np.bool_)) or not hasattr(val, "__float__"):
+                raise TypeError(f"'{type(val).__name__}' object cannot be converted to 'PyFloat'")
+            new["mass_tolerance"] = float(np.float32(float(val)))
+        if "top_k_fragments" in config:
+            val = config["top_k_fragments"]
+            if isinstance(val, (float, np.floating)) or not hasattr(val, "__index__"):
+                raise TypeError(f"'{type(val).__name__}' object cannot be interpreted as an integer")
+            iv = int(val.__index__())
+            if iv < 0:
+                raise OverflowError("can't convert negative int to unsigned")
+            new["top_k_fragments"] = iv
+        object.__setattr__(self, "_v", new)
+
+    def _c(self) -> F.AdsScoringParams:
+        p = F.AdsScoringParams()
+        p.mass_tolerance = self._v["mass_tolerance"]
+        p.top_k_fragments = min(self._v["top_k_fragments"], 2**63 - 1)
+        return p
+
+    def __repr__(self):
+        return "ScoringParameters(" + ", ".join(f"{k}={v!r}" for k, v in self._v.items()) + ")"
+
+
+def _feature_names() -> tuple:
+    names = (C.c_char_p * 64)()
+    n = _lib().ads_feature_names(names, 64)
+    return tuple(names[k].decode() for k in range(n))
+
+
+class CandidateFeatureCollection:
+    """CandidateFeatureCollection (src/candidate/features.rs:192-431)."""
+
+    def __init__(self):
+        self._h = None
+        self._n = 0
+        self._dict = None
+
+    def __del__(self):
+        _release(self, "ads_features_destroy")
+
+    @classmethod
+    def _from_handle(cls, h: int) -> "CandidateFeatureCollection":
+        c = cls()
+        c._h = h
+        c._n = int(_lib().ads_features_size(h))
+        return c
+
+    def len(self) -> int:
+        return self._n
+
+    def __len__(self) -> int:
+        return self._n
+
+    def is_empty(self) -> bool:
+        return self._n == 0
+
+    def to_dict_arrays(self) -> dict:
+        """precursor_idx and rank (uint64) and the 41 float32 feature columns
+        (src/candidate/features.rs:220-411)."""
+        if self._dict is None:
+            n = self._n
+            names = _feature_names()
+            pidx = np.zeros(max(n, 1), np.uint64)
+            rank = np.zeros(max(n, 1), np.uint64)
+            feats = np.zeros((len(names), max(n, 1)), np.float32)
+            if self._h is not None and n:
+                F.check(_lib().ads_features_copy_out(self._h, pidx.ctypes.data, rank.ctypes.data,
+                                                     feats.ctypes.data))
+            d = {"precursor_idx": pidx[:n], "rank": rank[:n]}
+            for k, name in enumerate(names):
+                d[name] = np.ascontiguousarray(feats[k, :n])
+            self._dict = d
+        return {k: v.copy() for k, v in self._dict.items()}
+
+    @staticmethod
+    def get_feature_names() -> list:
+        """src/candidate/features.rs:413-416"""
+        return list(_feature_names())
+
+
+class PeakGroupScoring:
+    """PeakGroupScoring (src/peak_group_scoring/mod.rs:29-101) on the GPU."""
+
+    def __init__(self, params: ScoringParameters, *, verbose: bool = True):
+        if not isinstance(params, ScoringParameters):
+            raise TypeError("argument 'params': expected ScoringParameters")
+        self.params = params
+        self.verbose = verbose
+
+    def score(self, dia_data: DIAData, lib: SpecLibFlat,
+              candidates: CandidateCollection) -> CandidateFeatureCollection:
+        if not isinstance(dia_data, DIAData) or not isinstance(lib, SpecLibFlat) or \
+                not isinstance(candidates, CandidateCollection):
+            raise TypeError("score(dia_data: DIAData, lib: SpecLibFlat, candidates: CandidateCollection)")
+        if dia_data._h is None or lib._h is None:
+            raise ValueError("DIAData and SpecLibFlat must be built with from_arrays")
+        p = self.params._c()
+        out = C.c_void_p()
+        L = _lib()
+        if candidates._h is not None and candidates._arrays is None:
+            F.check(L.ads_score(C.byref(p), dia_data._h, lib._h, candidates._h, int(self.verbose),
+                                C.byref(out)))
+        else:
+            a = candidates._materialize()
+            cols = [np.ascontiguousarray(a[k], np.uint64) for k in
+                    ("precursor_idx", "rank", "cycle_center", "cycle_start", "cycle_stop")]
+            sc = np.ascontiguousarray(a["score"], np.float32)
+            n = len(cols[0])
+            F.check(L.ads_score_arrays(C.byref(p), dia_data._h, lib._h, n, cols[0].ctypes.data,
+                                       cols[1].ctypes.data, sc.ctypes.data, cols[2].ctypes.data,
+                                       cols[3].ctypes.data, cols[4].ctypes.data, F.ADS_MEM_HOST,
+                                       int(self.verbose), C.byref(out)))
+        return CandidateFeatureCollection._from_handle(out.value)

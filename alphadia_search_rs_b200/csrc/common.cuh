@@ -286,10 +286,41 @@ struct AdsLib {
   float* ptol_p = nullptr;     // optional per-precursor RT half-window
   uint64_t* fstart_p = nullptr;
   uint64_t* fstop_p = nullptr;
+  uint8_t* naa_p = nullptr;    // precursor_naa (scoring), sorted like the other precursor arrays
   float* fmz_p = nullptr;      // fragment arrays, input order
+  float* fmzl_p = nullptr;     // fragment_mz_library (scoring's IDF)
   float* fint_p = nullptr;
   uint8_t* fnum_p = nullptr;
   uint8_t* ftype_p = nullptr;
   bool has_tol = false;
   float max_tol = 0.0f;
+  // InverseDocumentFrequency (src/idf/mod.rs:13-33): fragments of the library per
+  // m/z grid bin, built on the first scoring call
+  std::mutex mu;
+  ads::DevBuf<uint32_t> idf_counts;
 };
+
+// Candidate columns on the device (CandidateCollection, src/candidate/entry.rs:41-179).
+struct AdsCandidates {
+  int device = 0;
+  cudaEvent_t done = nullptr;
+  int64_t cap = -1;
+  ads::DevBuf<char> arena;  // all columns and counters in one allocation
+  uint64_t* pidx_p = nullptr;
+  uint64_t* rank_p = nullptr;
+  uint64_t* center_p = nullptr;
+  uint64_t* start_p = nullptr;
+  uint64_t* stop_p = nullptr;
+  float* score_p = nullptr;
+  int64_t* count_p = nullptr;
+  int* err_p = nullptr;
+  int64_t count = 0;
+  bool pending = false;
+  ~AdsCandidates() {
+    if (done) {
+      cudaEventSynchronize(done);
+      cudaEventDestroy(done);
+    }
+  }
+};
+

@@ -133,7 +133,9 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     lib->ptol_p = lib->has_tol ? c.take<float>(P) : nullptr;
     lib->fstart_p = c.take<uint64_t>(P);
     lib->fstop_p = c.take<uint64_t>(P);
+    lib->naa_p = c.take<uint8_t>(P);
     lib->fmz_p = c.take<float>(NF);
+    lib->fmzl_p = c.take<float>(NF);
     lib->fint_p = c.take<float>(NF);
     lib->fnum_p = c.take<uint8_t>(NF);
     lib->ftype_p = c.take<uint8_t>(NF);
@@ -150,6 +152,7 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
   float *pmz_in = nullptr, *prt_in = nullptr, *ptol_in = nullptr;
   uint64_t *fs_in = nullptr, *fe_in = nullptr;
   uint32_t *pos_in = nullptr, *pos_out = nullptr;
+  uint8_t* naa_in = nullptr;
   void* sort_tmp = nullptr;
   size_t sort_bytes = 0;
   const bool sort = P > 1;
@@ -164,6 +167,7 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
       ptol_in = lib->has_tol ? q.take<float>(P) : nullptr;
       fs_in = q.take<uint64_t>(P);
       fe_in = q.take<uint64_t>(P);
+      naa_in = q.take<uint8_t>(P);
       pos_in = q.take<uint32_t>(P);
       pos_out = q.take<uint32_t>(P);
       sort_tmp = q.take<char>((int64_t)sort_bytes);
@@ -181,7 +185,14 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
   ADS_TRY(copy_in(sort ? fs_in : lib->fstart_p, a->flat_frag_start_idx, P, L, st));
   ADS_TRY(copy_in(sort ? fe_in : lib->fstop_p, a->flat_frag_stop_idx, P, L, st));
   if (lib->has_tol) ADS_TRY(copy_in(sort ? ptol_in : lib->ptol_p, a->precursor_rt_tolerance, P, L, st));
+  if (a->precursor_naa)
+    ADS_TRY(copy_in(sort ? naa_in : lib->naa_p, a->precursor_naa, P, L, st));
+  else if (P)
+    ADS_CUDA(cudaMemsetAsync(sort ? naa_in : lib->naa_p, 0, (size_t)P, st));
   ADS_TRY(copy_in(lib->fmz_p, a->fragment_mz, NF, L, st));
+  // fragment_mz_library defaults to fragment_mz (the IDF of scoring reads it)
+  ADS_TRY(copy_in(lib->fmzl_p, a->fragment_mz_library ? a->fragment_mz_library : a->fragment_mz, NF,
+                  L, st));
   ADS_TRY(copy_in(lib->fint_p, a->fragment_intensity, NF, L, st));
   ADS_TRY(copy_in(lib->fnum_p, a->fragment_number, NF, L, st));
   ADS_TRY(copy_in(lib->ftype_p, a->fragment_type, NF, L, st));
@@ -196,6 +207,7 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     launch_gather(P, pos_out, prt_in, lib->prt_p, st);
     launch_gather(P, pos_out, fs_in, lib->fstart_p, st);
     launch_gather(P, pos_out, fe_in, lib->fstop_p, st);
+    launch_gather(P, pos_out, naa_in, lib->naa_p, st);
     if (lib->has_tol) launch_gather(P, pos_out, ptol_in, lib->ptol_p, st);
     ADS_LAUNCH_CHECK();
   }

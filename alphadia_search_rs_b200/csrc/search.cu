@@ -563,28 +563,6 @@ struct AdsSelection {
 // A candidate collection does not depend on the selection that filled it: the
 // search records `done` on the selection's stream, and every later read waits on
 // that event from the calling thread's per-thread stream.
-struct AdsCandidates {
-  int device = 0;
-  cudaEvent_t done = nullptr;
-  int64_t cap = -1;
-  ads::DevBuf<char> arena;  // all columns and counters in one allocation
-  uint64_t* pidx_p = nullptr;
-  uint64_t* rank_p = nullptr;
-  uint64_t* center_p = nullptr;
-  uint64_t* start_p = nullptr;
-  uint64_t* stop_p = nullptr;
-  float* score_p = nullptr;
-  int64_t* count_p = nullptr;
-  int* err_p = nullptr;
-  int64_t count = 0;
-  bool pending = false;
-  ~AdsCandidates() {
-    if (done) {
-      cudaEventSynchronize(done);
-      cudaEventDestroy(done);
-    }
-  }
-};
 
 namespace ads {
 namespace {

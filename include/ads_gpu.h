@@ -274,6 +274,44 @@ int ads_candidates_copy_out(AdsCandidates* cand, uint64_t* precursor_idx, uint64
                             uint64_t* cycle_stop);
 int ads_candidates_destroy(AdsCandidates* cand);
 
+/* ---------------------------------------------------------------- scoring */
+
+/* ScoringParameters (src/peak_group_scoring/parameters.rs:4-40). */
+typedef struct {
+  float mass_tolerance;    /* ppm; default 7.0 */
+  int64_t top_k_fragments; /* default 100 */
+} AdsScoringParams;
+void ads_scoring_params_default(AdsScoringParams* p);
+
+/* CandidateFeatureCollection (src/candidate/features.rs:192-431): 41 f32 features per
+ * candidate, device resident. */
+typedef struct AdsFeatures AdsFeatures;
+
+/* PeakGroupScoring.score (src/peak_group_scoring/mod.rs:42-101) of the candidates of a
+ * search (waits for that search).  Candidates whose precursor_idx is not in the library
+ * are left out, as in the reference; the others keep their order.  verbose: print the
+ * reference's "Scored N candidates at R candidates/second" line.  The library's IDF
+ * histogram (src/idf/mod.rs:13-33) is built on its first scoring call. */
+int ads_score(const AdsScoringParams* params, const AdsDia* dia, AdsLib* lib, AdsCandidates* cand,
+              int verbose, AdsFeatures** out);
+/* The same for candidate columns given as arrays (CandidateCollection.from_arrays),
+ * host or device memory.  Cycle ranges outside the run's RT index are an
+ * ADS_ERR_INVALID_ARGUMENT (the reference indexes out of bounds). */
+int ads_score_arrays(const AdsScoringParams* params, const AdsDia* dia, AdsLib* lib, int64_t n,
+                     const uint64_t* precursor_idx, const uint64_t* rank, const float* score,
+                     const uint64_t* cycle_center, const uint64_t* cycle_start,
+                     const uint64_t* cycle_stop, int location, int verbose, AdsFeatures** out);
+/* Scored candidates (rows that to_dict_arrays returns). */
+int64_t ads_features_size(const AdsFeatures* features);
+/* Copies into host arrays of ads_features_size() elements; `features` holds the 41
+ * columns one after another, in the order of ads_feature_names (CandidateFeatureCollection
+ * .get_feature_names, src/candidate/features.rs:6-48). */
+int ads_features_copy_out(const AdsFeatures* features, uint64_t* precursor_idx, uint64_t* rank,
+                          float* features_out);
+int ads_features_destroy(AdsFeatures* features);
+/* Writes up to cap feature names; returns their number (41). */
+int ads_feature_names(const char** names, int cap);
+
 #ifdef __cplusplus
 }
 #endif
