@@ -156,6 +156,7 @@ SIGNATURES = {
     "ads_score_arrays": (C.c_int, [C.POINTER(AdsScoringParams), vp, vp, i64, vp, vp, vp, vp, vp, vp,
                                    C.c_int, C.c_int, C.POINTER(vp)]),
     "ads_features_size": (i64, [vp]),
+    "ads_features_kernel_ms": (C.c_float, [vp]),
     "ads_features_copy_out": (C.c_int, [vp, vp, vp, vp]),
     "ads_features_destroy": (C.c_int, [vp]),
     "ads_feature_names": (C.c_int, [C.POINTER(C.c_char_p), C.c_int]),

@@ -298,6 +298,39 @@ class SpecLibFlat:
 
 _FLOAT_KEYS = ("fwhm_rt", "mass_tolerance", "rt_tolerance")
 _USIZE_KEYS = ("kernel_size", "peak_length", "candidate_count", "top_k_fragments")
+# the order in which update() reads the keys (parameters.rs:45-68)
+_SELECTION_UPDATE_ORDER = ("fwhm_rt", "kernel_size", "peak_length", "mass_tolerance", "rt_tolerance",
+                           "candidate_count", "top_k_fragments")
+
+
+def _extract_f32(val) -> float:
+    """pyo3's extract::<f32>: any object with __float__ (or __index__), rounded to f32."""
+    if not (hasattr(val, "__float__") or hasattr(val, "__index__")):
+        raise TypeError(f"'{type(val).__name__}' object cannot be converted to 'PyFloat'")
+    return float(np.float32(float(val)))
+
+
+def _extract_usize(val) -> int:
+    """pyo3's extract::<usize>: integers only (no floats), 0 <= v < 2**64."""
+    if isinstance(val, (float, np.floating)) or not hasattr(val, "__index__"):
+        raise TypeError(f"'{type(val).__name__}' object cannot be interpreted as an integer")
+    iv = int(val.__index__())
+    if iv < 0:
+        raise OverflowError("can't convert negative int to unsigned")
+    if iv >= 2**64:
+        raise OverflowError("int too big to convert")
+    return iv
+
+
+def _update_in_order(obj, config: dict, order) -> None:
+    """Reads the keys present in ``config`` in the reference's order; the first
+    value that does not convert raises, and the keys read before it stay set."""
+    for k in order:
+        if k in config:
+            conv = _extract_f32 if k in _FLOAT_KEYS else _extract_usize
+            v = dict(object.__getattribute__(obj, "_v"))
+            v[k] = conv(config[k])
+            object.__setattr__(obj, "_v", v)
 
 
 class SelectionParameters:
@@ -324,26 +357,7 @@ class SelectionParameters:
 
     def update(self, config: dict) -> None:
         """Sets any of the seven keys present in ``config`` (parameters.rs:45-68)."""
-        new = dict(self._v)
-        for k in _FLOAT_KEYS:
-            if k in config:
-                val = config[k]
-                if isinstance(val, (bool, np.bool_)) or not isinstance(val, (int, float, np.integer, np.floating)):
-                    if not hasattr(val, "__float__"):
-                        raise TypeError(f"'{type(val).__name__}' object cannot be converted to 'PyFloat'")
-                new[k] = float(np.float32(float(val)))
-        for k in _USIZE_KEYS:
-            if k in config:
-                val = config[k]
-                if isinstance(val, (float, np.floating)) or not hasattr(val, "__index__"):
-                    raise TypeError(f"'{type(val).__name__}' object cannot be interpreted as an integer")
-                iv = int(val.__index__())
-                if iv < 0:
-                    raise OverflowError("can't convert negative int to unsigned")
-                if iv >= 2**64:
-                    raise OverflowError("int too big to convert")
-                new[k] = iv
-        object.__setattr__(self, "_v", new)
+        _update_in_order(self, config, _SELECTION_UPDATE_ORDER)
 
     def _c(self) -> F.AdsSelectionParams:
         p = F.AdsSelectionParams()
@@ -611,21 +625,7 @@ class ScoringParameters:
 
     def update(self, config: dict) -> None:
         """Sets mass_tolerance and/or top_k_fragments (parameters.rs:28-37)."""
-        new = dict(self._v)
-        if "mass_tolerance" in config:
-            val = config["mass_tolerance"]
-            if isinstance(val, (bool, np.bool_)) or not hasattr(val, "__float__"):
-                raise TypeError(f"'{type(val).__name__}' object cannot be converted to 'PyFloat'")
-            new["mass_tolerance"] = float(np.float32(float(val)))
-        if "top_k_fragments" in config:
-            val = config["top_k_fragments"]
-            if isinstance(val, (float, np.floating)) or not hasattr(val, "__index__"):
-                raise TypeError(f"'{type(val).__name__}' object cannot be interpreted as an integer")
-            iv = int(val.__index__())
-            if iv < 0:
-                raise OverflowError("can't convert negative int to unsigned")
-            new["top_k_fragments"] = iv
-        object.__setattr__(self, "_v", new)
+        _update_in_order(self, config, ("mass_tolerance", "top_k_fragments"))
 
     def _c(self) -> F.AdsScoringParams:
         p = F.AdsScoringParams()
@@ -669,6 +669,10 @@ class CandidateFeatureCollection:
 
     def is_empty(self) -> bool:
         return self._n == 0
+
+    def kernel_ms(self) -> float:
+        """Extension: device time of the scoring kernel in milliseconds."""
+        return float(_lib().ads_features_kernel_ms(self._h)) if self._h is not None else 0.0
 
     def to_dict_arrays(self) -> dict:
         """precursor_idx and rank (uint64) and the 41 float32 feature columns

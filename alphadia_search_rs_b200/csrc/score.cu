@@ -39,6 +39,7 @@ struct AdsFeatures {
   float* feat_p = nullptr;  // feature k of row q at k * n + q
   uint8_t* found_p = nullptr;
   std::vector<uint8_t> found;
+  float kernel_ms = 0.0f;  // CUDA-event time of score_kernel
 };
 
 namespace ads {
@@ -623,7 +624,13 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
   DevBuf<int> err;
   ADS_TRY(err.alloc(1));
   ADS_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), st));
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  struct Events {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~Events() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } ev;
   if (n > 0) {
     const int Fm = (int)std::max<int64_t>(1, std::min<int64_t>(p->top_k_fragments, l->max_frag));
     const int Fraw = (int)std::max<int64_t>(1, l->max_frag);
@@ -678,14 +685,12 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
     a.o_feat = f->feat_p;
     a.o_found = f->found_p;
     a.err = err.p;
-    if (verbose) {
-      ADS_CUDA(cudaEventCreate(&e0));
-      ADS_CUDA(cudaEventCreate(&e1));
-      ADS_CUDA(cudaEventRecord(e0, st));
-    }
+    ADS_CUDA(cudaEventCreate(&ev.a));
+    ADS_CUDA(cudaEventCreate(&ev.b));
+    ADS_CUDA(cudaEventRecord(ev.a, st));
     score_kernel<<<(int)((T + kScoreBlock - 1) / kScoreBlock), kScoreBlock, 0, st>>>(a);
     ADS_LAUNCH_CHECK();
-    if (verbose) ADS_CUDA(cudaEventRecord(e1, st));
+    ADS_CUDA(cudaEventRecord(ev.b, st));
     f->found.resize((size_t)n);
     ADS_CUDA(cudaMemcpyAsync(f->found.data(), f->found_p, (size_t)n, cudaMemcpyDeviceToHost, st));
   }
@@ -697,14 +702,11 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
                 "candidate cycle range outside the run's RT index (or cycle_start > cycle_stop)");
   if (herr & 2) return fail(ADS_ERR_INTERNAL, "fragment count above the scratch plan");
   for (uint8_t v : f->found) f->count += v;
+  if (n > 0) ADS_CUDA(cudaEventElapsedTime(&f->kernel_ms, ev.a, ev.b));
   if (verbose && n > 0) {
-    float ms = 0.0f;
-    ADS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     // src/peak_group_scoring/mod.rs:91-98
     printf("Scored %lld candidates at %.2f candidates/second\n", (long long)n,
-           (double)n / std::max(1e-9, ms * 1e-3));
+           (double)n / std::max(1e-9, (double)f->kernel_ms * 1e-3));
     fflush(stdout);
   }
   *out = f.release();
@@ -799,6 +801,8 @@ int ads_score_arrays(const AdsScoringParams* params, const AdsDia* dia, AdsLib* 
 }
 
 int64_t ads_features_size(const AdsFeatures* f) { return f ? f->count : -1; }
+
+float ads_features_kernel_ms(const AdsFeatures* f) { return f ? f->kernel_ms : -1.0f; }
 
 int ads_features_copy_out(const AdsFeatures* f, uint64_t* precursor_idx, uint64_t* rank,
                           float* features) {

@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-windows", type=int, default=0,
                     help="MS2 windows in the CPU-baseline sample (0: about 72 M peaks' worth)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-scoring", action="store_true",
+                    help="skip the PeakGroupScoring figures added to the JSON line")
     ap.add_argument("--warps-per-block", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--cycles-per-lane", type=int, default=0)
@@ -272,6 +274,108 @@ def bf16_agreement(got: dict, ref: dict, eps_rel_max: float = 1e-3):
         den = max(abs(float(s64)), eps_rel_max * ref_max[int(p)])
         errs.append(abs(m[1] - float(s64)) / den if den > 0 else 0.0)
     return same / max(len(ref["rank"]), 1), np.asarray(errs if errs else [0.0])
+
+
+def sub_library_arrays(sub: dict) -> dict:
+    """SpecLibFlat.from_arrays keywords (numpy, reference dtypes) of a window
+    subset's library, with the same constant columns as library_tensors."""
+    P, NF = len(sub["precursor_idx"]), len(sub["fragment_mz"])
+    out = dict(
+        precursor_idx=sub["precursor_idx"], precursor_mz_library=sub["precursor_mz"],
+        precursor_mz=sub["precursor_mz"], precursor_rt_library=sub["precursor_rt"],
+        precursor_rt=sub["precursor_rt"], precursor_naa=np.full(P, 10, np.uint8),
+        flat_frag_start_idx=sub["flat_frag_start_idx"], flat_frag_stop_idx=sub["flat_frag_stop_idx"],
+        fragment_mz_library=sub["fragment_mz"], fragment_mz=sub["fragment_mz"],
+        fragment_intensity=sub["fragment_intensity"],
+        fragment_cardinality=np.ones(NF, np.uint8), fragment_charge=np.ones(NF, np.uint8),
+        fragment_loss_type=np.zeros(NF, np.uint8), fragment_number=sub["fragment_number"],
+        fragment_position=np.ones(NF, np.uint8), fragment_type=sub["fragment_type"])
+    if "rt_tolerance" in sub:
+        out["precursor_rt_tolerance"] = sub["rt_tolerance"]
+    return out
+
+
+def scoring_figures(ads, dia, slib, cand, out_np, steps: int = 3) -> dict:
+    """PeakGroupScoring.score of the search's candidates: the scoring kernel's device
+    time (CUDA events), the call on the device-resident collection, and end to end
+    from pinned host arrays to host feature arrays."""
+    import torch
+
+    scorer = ads.PeakGroupScoring(ads.ScoringParameters(), verbose=False)
+    scorer.score(dia, slib, cand)  # warm-up: IDF histogram of the library, scratch pool
+    k_ms, call_s = [], []
+    n = 0
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f = scorer.score(dia, slib, cand)
+        call_s.append(time.perf_counter() - t0)
+        k_ms.append(f.kernel_ms())
+        n = len(f)
+        del f
+    arrs = cand.to_arrays(out=out_np)
+    nc = len(arrs[0])
+    e2e_s = []
+    d2h = 0
+    for i in range(steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cc = ads.CandidateCollection.from_arrays(*arrs)
+        f = scorer.score(dia, slib, cc)
+        d = f.to_dict_arrays()
+        dt = time.perf_counter() - t0
+        d2h = len(f) * (2 * 8 + 4 * 41) + nc  # precursor_idx, rank, 41 features; found flags
+        del cc, f, d
+        if i > 0:
+            e2e_s.append(dt)
+    kms = statistics.median(k_ms)
+    return {"metric": "candidates scored per second (PeakGroupScoring.score, 41 features)",
+            "value": n / (kms / 1e3), "unit": "candidates/s", "candidates": int(n),
+            "kernel_ms": kms, "call_ms": 1e3 * statistics.median(call_s),
+            "call_value": n / statistics.median(call_s),
+            "e2e": {"value": n / statistics.median(e2e_s), "unit": "candidates/s",
+                    "h2d_bytes_per_step": int(nc * (5 * 8 + 4)), "d2h_bytes_per_step": int(d2h),
+                    "path": "CandidateCollection.from_arrays(pinned host arrays) + "
+                            "PeakGroupScoring.score + CandidateFeatureCollection.to_dict_arrays"},
+            "timing": f"median of {steps} calls after one warm-up"}
+
+
+def scoring_cpu_and_parity(ads, oracle, host: dict, sub: dict, od, ol, res: dict, n_threads: int,
+                           local_rank: int, steps: int = 3):
+    """The oracle's PeakGroupScoring on the CPU sample's candidates (timed), and the
+    device's features of the same candidates against it (correctly rounded logs:
+    every feature bit for bit)."""
+    la = sub_library_arrays(sub)
+    oracle.lib_set_scoring(ol, la["precursor_naa"], la["fragment_mz_library"])
+    cols = {k: res[k] for k in ("precursor_idx", "rank", "score", "cycle_center", "cycle_start",
+                                "cycle_stop")}
+    oracle.score(od, ol, cols, n_threads=n_threads)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        oracle.score(od, ol, cols, n_threads=n_threads)
+        ts.append(time.perf_counter() - t0)
+    nc = len(cols["rank"])
+    cpu = {"value": nc / statistics.mean(ts), "unit": "candidates/s", "cores": n_threads,
+           "kind": "port", "sample": f"the {nc} candidates of the search CPU sample, mean of "
+                                     f"{steps} timed calls"}
+    ref = oracle.score(od, ol, cols, log_mode=oracle.LOG_RN, n_threads=n_threads)
+    kw = dict(la)
+    tol = kw.pop("precursor_rt_tolerance", None)
+    dsub = ads.DIAData.from_arrays(*(host[k] for k in RUN_KEYS), host["cycle"], device=local_rank)
+    lsub = ads.SpecLibFlat.from_arrays(**kw, precursor_rt_tolerance=tol, device=local_rank)
+    z = np.zeros(nc, np.uint64)
+    cc = ads.CandidateCollection.from_arrays(cols["precursor_idx"], cols["rank"], cols["score"], z, z, z,
+                                             cols["cycle_center"], cols["cycle_start"], cols["cycle_stop"])
+    got = ads.PeakGroupScoring(ads.ScoringParameters(), verbose=False).score(dsub, lsub, cc).to_dict_arrays()
+    same_rows = len(got["rank"]) == len(ref["rank"]) and all(
+        np.array_equal(got[k], ref[k]) for k in ("precursor_idx", "rank"))
+    diff = [k for k in oracle.FEATURE_NAMES
+            if not same_rows or not np.array_equal(got[k].view(np.uint32), ref[k].view(np.uint32))]
+    parity = {"candidates": int(nc), "rows_identical": bool(same_rows),
+              "features_bit_identical": len(diff) == 0, "features_differing": diff}
+    del dsub, lsub, cc
+    return cpu, parity
 
 
 def oracle_setup(host: dict, sub: dict, n_threads: int):
@@ -549,6 +653,9 @@ def run_ours(args, rank, world, local_rank):
     #      parity spot check of the GPU result for the same precursors
     cpu = None
     parity = None
+    scoring = None
+    if world == 1 and not args.no_scoring:
+        scoring = scoring_figures(ads, dia, slib, cand, out_np)
     if world == 1 and not args.no_cpu_baseline:
         import oracle
 
@@ -574,6 +681,9 @@ def run_ours(args, rank, world, local_rank):
         parity = {"precursors": int(len(sub["precursor_idx"])), "candidates": int(len(res["rank"])),
                   "indices_identical": all(same.values()) and int(mask.sum()) == len(res["rank"]),
                   "max_score_rel_err_vs_glibc_logf": rel}
+        if scoring is not None:
+            scoring["cpu_baseline"], scoring["parity_sample"] = scoring_cpu_and_parity(
+                ads, oracle, host, sub, od, ol, res, n, local_rank)
         if precision == "bf16":
             # BF16 storage is compared with the FP64 oracle: top-K cycle agreement and
             # relative score error (against max(|s64|, 1e-3 * the precursor's largest |s64|))
@@ -613,6 +723,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline,
         "cpu_baseline": cpu,
         "parity_sample": parity,
+        "scoring": scoring,
         "clocks": clk.summary(),
         "setup_s": {"generate": t_gen, "dia_build": t_dia, "lib_build": t_lib},
         "counters": stats,

@@ -303,6 +303,11 @@ int ads_score_arrays(const AdsScoringParams* params, const AdsDia* dia, AdsLib* 
                      const uint64_t* cycle_stop, int location, int verbose, AdsFeatures** out);
 /* Scored candidates (rows that to_dict_arrays returns). */
 int64_t ads_features_size(const AdsFeatures* features);
+/* Device time of the scoring kernel that filled the handle, in milliseconds (CUDA
+ * events on the launching stream); 0 for an empty collection, -1 for a null handle.
+ * The reference prints the same figure as candidates per second
+ * (src/peak_group_scoring/mod.rs:91-98). */
+float ads_features_kernel_ms(const AdsFeatures* features);
 /* Copies into host arrays of ads_features_size() elements; `features` holds the 41
  * columns one after another, in the order of ads_feature_names (CandidateFeatureCollection
  * .get_feature_names, src/candidate/features.rs:6-48). */

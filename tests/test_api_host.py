@@ -40,6 +40,62 @@ def test_selection_parameter_errors():
     assert p.kernel_size == 20  # failed updates leave the object unchanged
 
 
+def test_selection_update_reads_keys_in_order():  # src/peak_group_selection/parameters.rs:45-68
+    p = ads.SelectionParameters()
+    with pytest.raises(TypeError):
+        p.update({"top_k_fragments": 7.5, "fwhm_rt": 4.0, "candidate_count": 9})
+    # fwhm_rt and candidate_count are read before the failing key
+    assert (p.fwhm_rt, p.candidate_count, p.top_k_fragments) == (4.0, 9, 12)
+    p.update({"fwhm_rt": True})  # extract::<f32> takes bool like int
+    assert p.fwhm_rt == 1.0
+
+
+def test_scoring_parameter_defaults():  # src/peak_group_scoring/parameters.rs:16-25
+    p = ads.ScoringParameters()
+    assert p.mass_tolerance == 7.0 and p.top_k_fragments == 100
+
+
+def test_scoring_parameter_update():  # src/peak_group_scoring/parameters.rs:28-37
+    p = ads.ScoringParameters()
+    p.update({"mass_tolerance": 12, "other": "ignored"})
+    assert p.mass_tolerance == 12.0 and p.top_k_fragments == 100
+    p.update({"mass_tolerance": 0.1, "top_k_fragments": np.int64(24)})
+    assert p.mass_tolerance == float(np.float32(0.1)) and p.top_k_fragments == 24
+    with pytest.raises(AttributeError):
+        p.mass_tolerance = 3.0
+    with pytest.raises(TypeError):
+        p.update({"mass_tolerance": 5.0, "top_k_fragments": 2.0})
+    assert (p.mass_tolerance, p.top_k_fragments) == (5.0, 24)  # set before the failing key
+    with pytest.raises(OverflowError):
+        p.update({"top_k_fragments": -3})
+    with pytest.raises(TypeError):
+        p.update({"mass_tolerance": "7"})
+
+
+def test_feature_names():  # src/candidate/features.rs:6-48, 413-416
+    import oracle
+
+    names = ads.CandidateFeatureCollection.get_feature_names()
+    assert names == list(oracle.FEATURE_NAMES) and len(names) == 41
+    assert names[0] == "score" and names[-1] == "num_over_50_top6_idf"
+
+
+def test_empty_feature_collection():
+    f = ads.CandidateFeatureCollection()
+    assert f.is_empty() and len(f) == 0 and f.len() == 0 and f.kernel_ms() == 0.0
+    d = f.to_dict_arrays()
+    assert list(d)[:2] == ["precursor_idx", "rank"] and len(d) == 43
+    assert d["precursor_idx"].dtype == np.uint64 and d["score"].dtype == np.float32
+
+
+def test_scoring_argument_types():
+    s = ads.PeakGroupScoring(ads.ScoringParameters(), verbose=False)
+    with pytest.raises(TypeError):
+        s.score(None, None, ads.CandidateCollection())
+    with pytest.raises(TypeError):
+        ads.PeakGroupScoring({"mass_tolerance": 7.0})
+
+
 def test_candidate_collection_roundtrip():  # src/candidate/tests.rs:104-156
     cols = dict(precursor_idxs=[1, 2], ranks=[10, 20], scores=[0.1, 0.2], scan_center=[11, 21],
                 scan_start=[12, 22], scan_stop=[13, 23], cycle_center=[14, 24], cycle_start=[15, 25],
