@@ -709,15 +709,18 @@ class PeakGroupScoring:
 
     def score(self, dia_data: DIAData, lib: SpecLibFlat,
               candidates: CandidateCollection) -> CandidateFeatureCollection:
+        """Features of every candidate whose precursor_idx is in ``lib``.  Extension:
+        ``candidates`` may also be a DeviceCandidates buffer (search_into)."""
         if not isinstance(dia_data, DIAData) or not isinstance(lib, SpecLibFlat) or \
-                not isinstance(candidates, CandidateCollection):
+                not isinstance(candidates, (CandidateCollection, DeviceCandidates)):
             raise TypeError("score(dia_data: DIAData, lib: SpecLibFlat, candidates: CandidateCollection)")
         if dia_data._h is None or lib._h is None:
             raise ValueError("DIAData and SpecLibFlat must be built with from_arrays")
         p = self.params._c()
         out = C.c_void_p()
         L = _lib()
-        if candidates._h is not None and candidates._arrays is None:
+        if isinstance(candidates, DeviceCandidates) or (candidates._h is not None and
+                                                         candidates._arrays is None):
             F.check(L.ads_score(C.byref(p), dia_data._h, lib._h, candidates._h, int(self.verbose),
                                 C.byref(out)))
         else:

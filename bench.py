@@ -295,6 +295,10 @@ def sub_library_arrays(sub: dict) -> dict:
     return out
 
 
+CAND_COLS = ("precursor_idx", "rank", "score", "scan_center", "scan_start", "scan_stop",
+             "cycle_center", "cycle_start", "cycle_stop")
+
+
 def scoring_figures(ads, dia, slib, cand, out_np, steps: int = 3) -> dict:
     """PeakGroupScoring.score of the search's candidates: the scoring kernel's device
     time (CUDA events), the call on the device-resident collection, and end to end
@@ -313,8 +317,8 @@ def scoring_figures(ads, dia, slib, cand, out_np, steps: int = 3) -> dict:
         k_ms.append(f.kernel_ms())
         n = len(f)
         del f
-    arrs = cand.to_arrays(out=out_np)
-    nc = len(arrs[0])
+    nc = cand.copy_out(dict(zip(CAND_COLS, out_np)))
+    arrs = tuple(o[:nc] for o in out_np)
     e2e_s = []
     d2h = 0
     for i in range(steps + 1):

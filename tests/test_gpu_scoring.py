@@ -188,3 +188,18 @@ def test_edge_case_library_bit_exact():
 
 def test_feature_names_match_reference_order():
     assert CandidateFeatureCollection.get_feature_names() == list(oracle.FEATURE_NAMES)
+
+
+def test_device_buffer_scores_like_collection(scored):
+    """A reusable DeviceCandidates buffer (search_into) is scored in place, twice in a
+    row, with the same features as the search's collection."""
+    s = scored
+    sel = PeakGroupSelection(params_from(s["cfg"].params_dict()), verbose=False)
+    buf = sel.new_candidates()
+    scorer = PeakGroupScoring(s["sp"], verbose=False)
+    for call in range(2):
+        sel.search_into(s["dia"], s["lib"], buf)
+        f = scorer.score(s["dia"], s["lib"], buf)
+        assert f.kernel_ms() > 0.0
+        assert_features_equal(f.to_dict_arrays(), s["got"], exact=True,
+                              where=f"{s['cfg'].name}/buffer/{call}")
