@@ -649,7 +649,6 @@ class CandidateFeatureCollection:
     def __init__(self):
         self._h = None
         self._n = 0
-        self._dict = None
 
     def __del__(self):
         _release(self, "ads_features_destroy")
@@ -677,20 +676,20 @@ class CandidateFeatureCollection:
     def to_dict_arrays(self) -> dict:
         """precursor_idx and rank (uint64) and the 41 float32 feature columns
         (src/candidate/features.rs:220-411)."""
-        if self._dict is None:
-            n = self._n
-            names = _feature_names()
-            pidx = np.zeros(max(n, 1), np.uint64)
-            rank = np.zeros(max(n, 1), np.uint64)
-            feats = np.zeros((len(names), max(n, 1)), np.float32)
-            if self._h is not None and n:
-                F.check(_lib().ads_features_copy_out(self._h, pidx.ctypes.data, rank.ctypes.data,
-                                                     feats.ctypes.data))
-            d = {"precursor_idx": pidx[:n], "rank": rank[:n]}
-            for k, name in enumerate(names):
-                d[name] = np.ascontiguousarray(feats[k, :n])
-            self._dict = d
-        return {k: v.copy() for k, v in self._dict.items()}
+        # fresh arrays on every call (as the reference builds them from its vectors):
+        # one device-to-host copy, the feature columns are rows of one block
+        n = self._n
+        names = _feature_names()
+        pidx = np.empty(max(n, 1), np.uint64)
+        rank = np.empty(max(n, 1), np.uint64)
+        feats = np.empty((len(names), max(n, 1)), np.float32)
+        if self._h is not None and n:
+            F.check(_lib().ads_features_copy_out(self._h, pidx.ctypes.data, rank.ctypes.data,
+                                                 feats.ctypes.data))
+        d = {"precursor_idx": pidx[:n], "rank": rank[:n]}
+        for k, name in enumerate(names):
+            d[name] = feats[k, :n]
+        return d
 
     @staticmethod
     def get_feature_names() -> list:

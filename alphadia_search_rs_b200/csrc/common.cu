@@ -59,6 +59,19 @@ int device_pool(int device, DevicePool* out) {
   *out = dp;
   return ADS_OK;
 }
+// The pool's release threshold counts all memory it holds, in use or not; keeping it
+// at (bytes in use + kPoolKeepBytes) keeps up to kPoolKeepBytes of freed memory for
+// reuse however much long-lived data (a run, a library) the pool holds.
+void update_release_threshold(cudaMemPool_t pool) {
+  uint64_t used = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  uint64_t keep = used + kPoolKeepBytes;
+  if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+    cudaGetLastError();
+}
 }  // namespace
 
 int pool_alloc(int device, size_t bytes, void** out) {
@@ -71,6 +84,7 @@ int pool_alloc(int device, size_t bytes, void** out) {
     *out = nullptr;
     return cuda_fail(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
   }
+  update_release_threshold(dp.pool);
   return ADS_OK;
 }
 
@@ -80,6 +94,7 @@ void pool_free(int device, void* p) {
   DeviceGuard dg(device);
   cudaDeviceSynchronize();  // nothing in flight may still read or write p
   cudaFreeAsync(p, dp.stream);
+  update_release_threshold(dp.pool);
   cudaStreamSynchronize(dp.stream);
   cudaGetLastError();
 }

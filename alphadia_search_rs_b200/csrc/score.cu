@@ -811,6 +811,12 @@ int ads_features_copy_out(const AdsFeatures* f, uint64_t* precursor_idx, uint64_
     if (f->n == 0) return ADS_OK;
     DeviceGuard dg(f->device);
     const size_t n = (size_t)f->n;
+    if (f->count == f->n) {  // every candidate scored: the device layout is the output's
+      if (precursor_idx) ADS_CUDA(cudaMemcpy(precursor_idx, f->pidx_p, n * 8, cudaMemcpyDeviceToHost));
+      if (rank) ADS_CUDA(cudaMemcpy(rank, f->rank_p, n * 8, cudaMemcpyDeviceToHost));
+      if (features) ADS_CUDA(cudaMemcpy(features, f->feat_p, n * 4 * kFeatures, cudaMemcpyDeviceToHost));
+      return ADS_OK;
+    }
     std::vector<uint64_t> p(n), r(n);
     std::vector<float> x(n * kFeatures);
     ADS_CUDA(cudaMemcpy(p.data(), f->pidx_p, n * 8, cudaMemcpyDeviceToHost));

@@ -203,3 +203,18 @@ def test_device_buffer_scores_like_collection(scored):
         assert f.kernel_ms() > 0.0
         assert_features_equal(f.to_dict_arrays(), s["got"], exact=True,
                               where=f"{s['cfg'].name}/buffer/{call}")
+
+
+def test_whole_run_cycle_ranges(scored):
+    """Candidates spanning the whole run (a scratch of several thousand words per
+    candidate) still match the oracle."""
+    s = scored
+    n_rt = len(s["od"].rt)
+    c = {k: v[:64].copy() for k, v in s["cand"].items()}
+    c["cycle_start"][:] = 0
+    c["cycle_stop"][:] = n_rt
+    c["cycle_center"][:] = np.minimum(c["cycle_center"], n_rt - 1)
+    got = PeakGroupScoring(s["sp"], verbose=False).score(
+        s["dia"], s["lib"], CandidateCollection.from_arrays(*(c[k] for k in COLS)))
+    ref = oracle.score(s["od"], s["ol"], c, log_mode=oracle.LOG_RN)
+    assert_features_equal(got.to_dict_arrays(), ref, exact=True, where=s["cfg"].name + "/long")
