@@ -542,11 +542,11 @@ class PeakGroupSelection:
         F.check(_lib().ads_selection_set_stats(self._h, 1 if on else 0))
 
     def last_stats(self) -> dict:
-        out = np.zeros(6, np.int64)
-        F.check(_lib().ads_selection_last_stats(self._h, out.ctypes.data, 6))
+        out = np.zeros(7, np.int64)
+        F.check(_lib().ads_selection_last_stats(self._h, out.ctypes.data, 7))
         return dict(pairs=int(out[0]), bins_plus_one=int(out[1]), fragments=int(out[2]),
                     entries_read=int(out[3]), entries_accumulated=int(out[4]),
-                    offsets_read=int(out[5]))
+                    offsets_read=int(out[5]), xic_cells=int(out[6]))
 
 
 class DeviceCandidates:

@@ -266,6 +266,20 @@ __device__ int select_fragments(const PrepArgs& a, int64_t p, int lane, uint8_t*
   return F;
 }
 
+// Statistics pass: sum over searched precursors of (kept fragments x cycles), the
+// XIC cells the convolution and the score visit.
+__global__ void cells_kernel(int64_t n, const int* nf, const int* cs, const int* ce,
+                             unsigned long long* out) {
+  unsigned long long v = 0;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int C = ce[p] - cs[p];
+    if (nf[p] > 0 && C > 0) v += (unsigned long long)nf[p] * (unsigned long long)C;
+  }
+  for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(out, v);
+}
+
 __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a) {
   extern __shared__ __align__(16) unsigned char prep_smem[];
   const int lane = threadIdx.x & 31;
@@ -338,6 +352,7 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a) {
 constexpr int kLaneCycles[] = {4, 8, 10, 12, 16};
 constexpr int kDefaultWarpsPerBlock = 4;
 constexpr int kMaxClasses = 10;
+constexpr int kStats = 7;  // statistics-pass counters (ads_selection_last_stats)
 
 // Length classes of one search: class b covers C <= bound[b] with S[b] cycles per
 // lane (bound[last] = the longest window, searched in one or more passes).
@@ -539,7 +554,7 @@ struct AdsSelection {
   int64_t last_launches = 0;
   bool stats_on = false;
   ads::DevBuf<unsigned long long> stats;
-  int64_t last_stats[6] = {0, 0, 0, 0, 0, 0};
+  int64_t last_stats[ads::kStats] = {0, 0, 0, 0, 0, 0, 0};
   // workspace
   ads::DevBuf<int> nf, cs, ce, nwin, wins, cand_n, cand_center;
   ads::DevBuf<float> fw, cand_score;
@@ -742,8 +757,8 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
   const int64_t nb = (P + kScanBlock - 1) / kScanBlock;
   ADS_TRY(s->block_sums.reserve((size_t)nb));
   if (s->stats_on) {
-    ADS_TRY(s->stats.reserve(6));
-    ADS_CUDA(cudaMemsetAsync(s->stats.p, 0, 6 * sizeof(unsigned long long), st));
+    ADS_TRY(s->stats.reserve(kStats));
+    ADS_CUDA(cudaMemsetAsync(s->stats.p, 0, kStats * sizeof(unsigned long long), st));
   }
 
   GridView g;
@@ -800,6 +815,12 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     prep_kernel<<<(int)prep_blocks, kPrepThreads, prep_smem, st>>>(pa);
     ADS_LAUNCH_CHECK();
     ++launches;
+    if (s->stats_on && P > 0) {
+      cells_kernel<<<(int)std::min<int64_t>((P + 255) / 256, 1184), 256, 0, st>>>(
+          P, s->nf.p, s->cs.p, s->ce.p, s->stats.p + 6);
+      ADS_LAUNCH_CHECK();
+      ++launches;
+    }
   }
 
   const double2* ln_tab = nullptr;
@@ -1198,11 +1219,11 @@ int ads_selection_last_stats(AdsSelection* s, int64_t* out, int64_t cap) {
     if (!s || !out) return fail(ADS_ERR_INVALID_ARGUMENT, "null argument");
     if (!s->stats_on || !s->stats.p) return fail(ADS_ERR_INVALID_ARGUMENT, "statistics not enabled");
     DeviceGuard dg(s->device);
-    unsigned long long v[6];
+    unsigned long long v[kStats];
     cudaStream_t st = s->o.stream ? (cudaStream_t)s->o.stream : s->stream;
     ADS_CUDA(cudaMemcpyAsync(v, s->stats.p, sizeof(v), cudaMemcpyDeviceToHost, st));
     ADS_CUDA(cudaStreamSynchronize(st));
-    for (int i = 0; i < 6 && i < cap; ++i) out[i] = (int64_t)v[i];
+    for (int i = 0; i < kStats && i < cap; ++i) out[i] = (int64_t)v[i];
     return ADS_OK;
   });
 }

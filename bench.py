@@ -642,6 +642,9 @@ def run_ours(args, rank, world, local_rank):
     gather_bytes = 4 * stats["bins_plus_one"] + (2 + s_i) * stats["entries_accumulated"]
     path_bytes = 8 * P + 8 * nf_raw + gather_bytes + 68 * n_cand
     peak, peak_kind = measured_peak()
+    h = len(sel.kernel()) // 2
+    dense_flops = stats.get("xic_cells", 0) * (3 * h + 2)
+    fp32_peak = 148 * 128 * 2 * (clk.summary().get("sm_max_mhz") or 1965) * 1e6 / 1e12
     achieved = gather_bytes / (search_ms / 1e3) / 1e9
     traffic = load_traffic(cfg.name)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -651,6 +654,12 @@ def run_ours(args, rank, world, local_rank):
                 "kernel_ms_per_launch": search_ms,
                 "path_bytes_per_step": path_bytes,
                 "path_gbs": path_bytes / (ms_max / args.steps / 1e3) / 1e9,
+                # the stencil and score work: XIC cells x (3h + 2) flops, h the kernel's
+                # half width; against the FP32 CUDA-core peak (148 SMs x 128 lanes x 2 x
+                # the max SM clock)
+                "dense_flops_per_launch": dense_flops,
+                "dense_tflops": dense_flops / (search_ms / 1e3) / 1e12,
+                "fp32_peak_tflops_nominal": fp32_peak,
                 "stage_ms": {"prep": prep_ms, "search": search_ms, "compaction": comp_ms}}
 
     # ---- CPU baseline (oracle port on the host cores, bounded sample) and a

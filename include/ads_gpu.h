@@ -240,7 +240,8 @@ int64_t ads_selection_stream(const AdsSelection* sel);
 int64_t ads_selection_last_launches(const AdsSelection* sel);
 /* Per-search counters of the last search: [0] (fragment, window) pairs gathered,
  * [1] sum over those pairs of (m/z bins + 1), [2] fragments searched, [3] XIC peak
- * entries read, [4] XIC peak entries accumulated (n_in), [5] CSR offsets read.
+ * entries read, [4] XIC peak entries accumulated (n_in), [5] CSR offsets read,
+ * [6] XIC cells convolved and scored (sum of kept fragments x cycles).
  * Collected only while enabled with ads_selection_set_stats. */
 int ads_selection_set_stats(AdsSelection* sel, int enabled);
 int ads_selection_last_stats(AdsSelection* sel, int64_t* out, int64_t cap);

@@ -213,3 +213,22 @@ def test_verbose_prints_reference_lines(capfd):
     out = capfd.readouterr().out
     assert "Precursors per second:" in out
     assert f"Found {cand.len()} candidates" in out
+
+
+def test_statistics_pass_counts(workload):
+    """The statistics pass: every searched fragment row spans at least one and at most
+    all cycles, and each accumulated entry was read."""
+    cfg, run, la, _ = workload
+    from alphadia_search_rs_b200 import PeakGroupSelection
+
+    from _util import params_from
+
+    _, dia, lib, _ = product_search(run, la, cfg.params_dict())
+    sel = PeakGroupSelection(params_from(cfg.params_dict()), verbose=False)
+    sel.enable_stats(True)
+    sel.search(dia, lib)
+    st = sel.last_stats()
+    n_cycles = len(dia.rt_index()[0])
+    assert st["fragments"] > 0
+    assert st["fragments"] <= st["xic_cells"] <= st["fragments"] * n_cycles
+    assert st["entries_accumulated"] <= st["entries_read"]
