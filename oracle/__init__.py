@@ -110,6 +110,11 @@ def lib():
         "orc_features_len": (_i64, [vp]),
         "orc_features_copy": (None, [vp, _u64p, _u64p, _f32p]),
         "orc_features_free": (None, [vp]),
+        "orc_quantify": (vp, [vp, vp, _f32, _i64, _u64p, _u64p, _u64p, _u64p, _u64p, _i64, C.c_int]),
+        "orc_quant_sizes": (None, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "orc_quant_copy": (None, [vp, _u64p, _u64p, _u64p, _f32p, _u64p, _u64p, _u64p, _f32p, _f32p,
+                                  _f32p, _f32p, _u64p, _u64p]),
+        "orc_quant_free": (None, [vp]),
         "orc_sc_normalize_profiles": (None, [_f32p, _i64, _i64, _i64, _f32p]),
         "orc_sc_median_axis0": (None, [_f32p, _i64, _i64, C.c_int, _f32p]),
         "orc_sc_correlation": (_f32, [_f32p, _f32p, _i64]),
@@ -484,6 +489,55 @@ def score(dia: "Dia", lb: "Lib", candidates: dict, mass_tolerance: float = 7.0,
     for k, name in enumerate(FEATURE_NAMES):
         out[name] = np.ascontiguousarray(feats[:m, k])
     return out
+
+
+QUANT_PRECURSOR_KEYS = ("precursor_idx", "mz_library", "mz", "rt_library", "rt", "naa", "rank",
+                        "rt_observed", "flat_frag_start_idx", "flat_frag_stop_idx")
+QUANT_FRAGMENT_KEYS = ("mz_library", "mz", "intensity", "cardinality", "charge", "loss_type", "number",
+                       "position", "type", "mz_observed", "correlation_observed", "mass_error_observed",
+                       "precursor_idx", "rank")
+
+
+def quantify(dia: "Dia", lb: "Lib", candidates: dict, library: dict, tolerance_ppm: float = 7.0,
+             top_k_fragments: int = 10000, n_threads: int = 0):
+    """PeakGroupQuantification.quantify (src/peak_group_quantification/mod.rs:49-168) as
+    SpecLibFlatQuantified.to_dict_arrays (src/speclib_flat_quantified/mod.rs:110-210):
+    (precursor dict, fragment dict).  ``library`` holds the SpecLibFlat.from_arrays
+    inputs, from which the pass-through columns are taken."""
+    L = lib()
+    n = len(candidates["precursor_idx"])
+    cols = [np.ascontiguousarray(candidates[k], np.uint64) for k in
+            ("precursor_idx", "rank", "cycle_center", "cycle_start", "cycle_stop")]
+    if n == 0:
+        cols = [np.zeros(1, np.uint64)] * 5
+    h = L.orc_quantify(dia._h, lb._h, float(tolerance_ppm), int(min(top_k_fragments, 2**63 - 1)),
+                       *cols, n, int(n_threads or os.cpu_count() or 1))
+    try:
+        np_, nf_ = C.c_int64(), C.c_int64()
+        L.orc_quant_sizes(h, C.byref(np_), C.byref(nf_))
+        P, NF = np_.value, nf_.value
+        pu = [np.zeros(max(P, 1), np.uint64) for _ in range(5)]
+        prt = np.zeros(max(P, 1), np.float32)
+        fu = [np.zeros(max(NF, 1), np.uint64) for _ in range(3)]
+        ff = [np.zeros(max(NF, 1), np.float32) for _ in range(4)]
+        L.orc_quant_copy(h, pu[0], pu[1], pu[2], prt, pu[3], pu[4], fu[0], ff[0], ff[1], ff[2], ff[3],
+                         fu[1], fu[2])
+    finally:
+        L.orc_quant_free(h)
+    prow, frow = pu[1][:P].astype(np.int64), fu[0][:NF].astype(np.int64)
+    g = lambda k, rows: np.asarray(library[k])[rows]
+    prec = {"precursor_idx": pu[0][:P], "mz_library": g("precursor_mz_library", prow),
+            "mz": g("precursor_mz", prow), "rt_library": g("precursor_rt_library", prow),
+            "rt": g("precursor_rt", prow), "naa": g("precursor_naa", prow), "rank": pu[2][:P],
+            "rt_observed": prt[:P], "flat_frag_start_idx": pu[3][:P], "flat_frag_stop_idx": pu[4][:P]}
+    frag = {"mz_library": g("fragment_mz_library", frow), "mz": g("fragment_mz", frow),
+            "intensity": ff[0][:NF], "cardinality": g("fragment_cardinality", frow),
+            "charge": g("fragment_charge", frow), "loss_type": g("fragment_loss_type", frow),
+            "number": g("fragment_number", frow), "position": g("fragment_position", frow),
+            "type": g("fragment_type", frow), "mz_observed": ff[1][:NF],
+            "correlation_observed": ff[2][:NF], "mass_error_observed": ff[3][:NF],
+            "precursor_idx": fu[1][:NF], "rank": fu[2][:NF]}
+    return prec, frag
 
 
 def sc_normalize_profiles(x, dilations: int = 1) -> np.ndarray:

@@ -1018,6 +1018,63 @@ void score_candidate(const OrcDia& d, const OrcLib& l, const Idf& idf, float tol
   o[40] = (float)count_above(c, F, 0.50f, m6.get());
 }
 
+
+// ---- PeakGroupQuantification (src/peak_group_quantification/mod.rs:49-168)
+
+struct OrcQuantFrag {
+  uint64_t frow;  // input position of the fragment in the library arrays
+  float intensity, mz_observed, correlation, mass_error;
+};
+
+struct OrcQuantRow {
+  bool ok = false;
+  uint64_t pidx = 0, prow = 0, rank = 0;
+  float rt_observed = 0.0f;
+  std::vector<OrcQuantFrag> frags;
+};
+
+// quantify_precursor (src/peak_group_quantification/mod.rs:88-167) for one candidate
+// whose precursor sits at sorted position i; false when the reference returns None.
+bool quantify_candidate(const OrcDia& d, const OrcLib& l, float tol, int64_t top_k, int64_t i,
+                        uint64_t pidx, uint64_t rank, uint64_t center, uint64_t cstart,
+                        uint64_t cstop, OrcQuantRow& out) {
+  if (cstop <= cstart || center < cstart || center >= cstop) return false;
+  if (center >= d.rt.size()) return false;  // the reference indexes out of bounds
+  const int64_t s = (int64_t)l.frag_start[(size_t)i], e = (int64_t)l.frag_stop[(size_t)i];
+  auto keep = filter_sort_fragments(e - s, l.fragment_mz.data() + s, l.fragment_intensity.data() + s,
+                                    l.fragment_number.data() + s, l.fragment_type.data() + s,
+                                    true, true, top_k);
+  const int64_t F = (int64_t)keep.size();
+  std::vector<float> fmz;
+  for (auto k : keep) fmz.push_back(l.fragment_mz[(size_t)(s + k)]);
+  const int64_t C = (int64_t)(cstop - cstart);
+  std::vector<float> xic((size_t)(F * C)), mzo((size_t)(F * C)), norm((size_t)(F * C));
+  dense_xic_mz(d, l.precursor_mz[(size_t)i], (int64_t)cstart, (int64_t)cstop, tol, fmz.data(), F,
+               xic.data(), mzo.data());
+  std::vector<float> mz_obs((size_t)F), err((size_t)F);
+  fragment_mz_errors(mzo.data(), xic.data(), F, C, fmz.data(), mz_obs.data(), err.data());
+  normalize_profiles(xic.data(), F, C, 1, norm.data());
+  auto nz = non_zero_rows(norm.data(), F, C);
+  std::vector<float> med_f((size_t)C);
+  median_axis_0(norm.data(), nz, C, med_f.data());  // filter_non_zero + median_axis_0
+  out.ok = false;
+  out.frags.clear();
+  for (int64_t f = 0; f < F; ++f) {
+    const float corr = correlation_safe(norm.data() + f * C, med_f.data(), C);
+    const float obs = ndarray_sum(xic.data() + f * C, C);
+    if (obs > 0.0f)  // PrecursorQuantified::filter_fragments_by_intensity(0.0)
+      out.frags.push_back({(uint64_t)(s + keep[(size_t)f]), obs, mz_obs[(size_t)f], corr,
+                           err[(size_t)f]});
+  }
+  if (out.frags.empty()) return false;
+  out.ok = true;
+  out.pidx = pidx;
+  out.prow = (uint64_t)l.order[(size_t)i];
+  out.rank = rank;
+  out.rt_observed = d.rt[(size_t)center];
+  return true;
+}
+
 }  // namespace
 
 struct OrcFeatures {
@@ -1309,6 +1366,95 @@ void orc_features_copy(const OrcFeatures* r, uint64_t* pidx, uint64_t* rank, flo
 }
 
 void orc_features_free(OrcFeatures* r) { delete r; }
+
+// SpecLibFlatQuantified::from_precursor_quantified_vec (src/speclib_flat_quantified/mod.rs:
+// 212-333): fragments in candidate order, precursors stably sorted by precursor_idx with
+// their fragment ranges.
+struct OrcQuant {
+  std::vector<uint64_t> p_idx, p_row, p_rank, p_start, p_stop;
+  std::vector<float> p_rt_observed;
+  std::vector<uint64_t> f_row, f_pidx, f_rank;
+  std::vector<float> f_intensity, f_mz_observed, f_correlation, f_mass_error;
+};
+
+OrcQuant* orc_quantify(const OrcDia* d, const OrcLib* l, float tolerance_ppm, int64_t top_k,
+                       const uint64_t* pidx, const uint64_t* rank, const uint64_t* center,
+                       const uint64_t* start, const uint64_t* stop, int64_t n, int n_threads) {
+  std::vector<OrcQuantRow> rows((size_t)n);
+  const int64_t P = (int64_t)l->precursor_idx.size();
+  const uint64_t* keys = l->precursor_idx.data();
+  parallel_for(n, n_threads, 64, [&](int64_t q) {
+    const uint64_t x = pidx[q];
+    int64_t i = rust_bsearch(
+        P, [&](int64_t m) { return keys[m] > x; }, [&](int64_t m) { return keys[m] == x; },
+        [&](int64_t m) { return keys[m] < x; });
+    if (i >= P || keys[i] != x) return;  // get_precursor_by_idx_filtered: None
+    quantify_candidate(*d, *l, tolerance_ppm, top_k, i, x, rank[q], center[q], start[q], stop[q],
+                       rows[(size_t)q]);
+  });
+  auto* r = new OrcQuant();
+  std::vector<size_t> kept;
+  uint64_t at = 0;
+  std::vector<uint64_t> fs, fe;
+  for (size_t q = 0; q < rows.size(); ++q) {
+    const auto& w = rows[q];
+    if (!w.ok) continue;
+    kept.push_back(q);
+    fs.push_back(at);
+    for (const auto& f : w.frags) {
+      r->f_row.push_back(f.frow);
+      r->f_intensity.push_back(f.intensity);
+      r->f_mz_observed.push_back(f.mz_observed);
+      r->f_correlation.push_back(f.correlation);
+      r->f_mass_error.push_back(f.mass_error);
+      r->f_pidx.push_back(w.pidx);
+      r->f_rank.push_back(w.rank);
+    }
+    at += w.frags.size();
+    fe.push_back(at);
+  }
+  std::vector<size_t> ord(kept.size());
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(),
+                   [&](size_t a, size_t b) { return rows[kept[a]].pidx < rows[kept[b]].pidx; });
+  for (size_t k : ord) {
+    const auto& w = rows[kept[k]];
+    r->p_idx.push_back(w.pidx);
+    r->p_row.push_back(w.prow);
+    r->p_rank.push_back(w.rank);
+    r->p_rt_observed.push_back(w.rt_observed);
+    r->p_start.push_back(fs[k]);
+    r->p_stop.push_back(fe[k]);
+  }
+  return r;
+}
+
+void orc_quant_sizes(const OrcQuant* r, int64_t* n_prec, int64_t* n_frag) {
+  *n_prec = (int64_t)r->p_idx.size();
+  *n_frag = (int64_t)r->f_row.size();
+}
+
+void orc_quant_copy(const OrcQuant* r, uint64_t* p_idx, uint64_t* p_row, uint64_t* p_rank,
+                    float* p_rt_observed, uint64_t* p_start, uint64_t* p_stop, uint64_t* f_row,
+                    float* f_intensity, float* f_mz_observed, float* f_correlation,
+                    float* f_mass_error, uint64_t* f_pidx, uint64_t* f_rank) {
+  auto cp = [](const auto& v, auto* dst) { std::copy(v.begin(), v.end(), dst); };
+  cp(r->p_idx, p_idx);
+  cp(r->p_row, p_row);
+  cp(r->p_rank, p_rank);
+  cp(r->p_rt_observed, p_rt_observed);
+  cp(r->p_start, p_start);
+  cp(r->p_stop, p_stop);
+  cp(r->f_row, f_row);
+  cp(r->f_intensity, f_intensity);
+  cp(r->f_mz_observed, f_mz_observed);
+  cp(r->f_correlation, f_correlation);
+  cp(r->f_mass_error, f_mass_error);
+  cp(r->f_pidx, f_pidx);
+  cp(r->f_rank, f_rank);
+}
+
+void orc_quant_free(OrcQuant* r) { delete r; }
 
 // ---- the scoring helpers on raw arrays (for the reference's unit-test values)
 

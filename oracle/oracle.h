@@ -161,6 +161,21 @@ OrcFeatures* orc_score(const OrcDia* d, const OrcLib* l, float mass_tolerance, i
 int64_t orc_features_len(const OrcFeatures* r);
 void orc_features_copy(const OrcFeatures* r, uint64_t* precursor_idx, uint64_t* rank, float* feats);
 void orc_features_free(OrcFeatures* r);
+
+// PeakGroupQuantification.quantify (src/peak_group_quantification/mod.rs:49-168) into the
+// SpecLibFlatQuantified layout (src/speclib_flat_quantified/mod.rs:212-333): precursor
+// rows (stably sorted by precursor_idx) and fragment rows (candidate order), with the
+// input rows of the library's precursor and fragment arrays for the pass-through columns.
+typedef struct OrcQuant OrcQuant;
+OrcQuant* orc_quantify(const OrcDia* d, const OrcLib* l, float tolerance_ppm, int64_t top_k,
+                       const uint64_t* pidx, const uint64_t* rank, const uint64_t* center,
+                       const uint64_t* start, const uint64_t* stop, int64_t n, int n_threads);
+void orc_quant_sizes(const OrcQuant* r, int64_t* n_prec, int64_t* n_frag);
+void orc_quant_copy(const OrcQuant* r, uint64_t* p_idx, uint64_t* p_row, uint64_t* p_rank,
+                    float* p_rt_observed, uint64_t* p_start, uint64_t* p_stop, uint64_t* f_row,
+                    float* f_intensity, float* f_mz_observed, float* f_correlation,
+                    float* f_mass_error, uint64_t* f_pidx, uint64_t* f_rank);
+void orc_quant_free(OrcQuant* r);
 /* the scoring helpers, for the reference's unit-test values */
 void orc_sc_normalize_profiles(const float* x, int64_t rows, int64_t cols, int64_t dil, float* out);
 void orc_sc_median_axis0(const float* x, int64_t rows, int64_t cols, int non_zero_only, float* out);
