@@ -93,6 +93,13 @@ class AdsScoringParams(C.Structure):
     ]
 
 
+class AdsQuantParams(C.Structure):
+    _fields_ = [
+        ("tolerance_ppm", f32),
+        ("top_k_fragments", i64),
+    ]
+
+
 class AdsEngineOptions(C.Structure):
     _fields_ = [
         ("precision", i32),
@@ -160,6 +167,14 @@ SIGNATURES = {
     "ads_features_copy_out": (C.c_int, [vp, vp, vp, vp]),
     "ads_features_destroy": (C.c_int, [vp]),
     "ads_feature_names": (C.c_int, [C.POINTER(C.c_char_p), C.c_int]),
+    "ads_quant_params_default": (None, [C.POINTER(AdsQuantParams)]),
+    "ads_quantify": (C.c_int, [C.POINTER(AdsQuantParams), vp, vp, vp, C.c_int, C.POINTER(vp)]),
+    "ads_quantify_arrays": (C.c_int, [C.POINTER(AdsQuantParams), vp, vp, i64, vp, vp, vp, vp, vp,
+                                      C.c_int, C.c_int, C.POINTER(vp)]),
+    "ads_quant_sizes": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i64)]),
+    "ads_quant_kernel_ms": (C.c_float, [vp]),
+    "ads_quant_copy_out": (C.c_int, [vp] + [vp] * 13),
+    "ads_quant_destroy": (C.c_int, [vp]),
 }
 
 _lib = None

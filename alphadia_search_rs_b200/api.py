@@ -218,10 +218,17 @@ class DIAData:
                     cycle_indices=cy[:n], intensities=it[:n])
 
 
+_QUANT_PASSTHROUGH = ("precursor_mz_library", "precursor_mz", "precursor_rt_library", "precursor_rt",
+                      "precursor_naa", "fragment_mz_library", "fragment_mz", "fragment_cardinality",
+                      "fragment_charge", "fragment_loss_type", "fragment_number", "fragment_position",
+                      "fragment_type")
+
+
 class SpecLibFlat:
     """SpecLibFlat (src/speclib_flat/mod.rs:6-199), device resident."""
 
     def __init__(self):
+        self._passthrough = None
         self._h = None
         self._n_prec = 0
         self._n_frag = 0
@@ -285,6 +292,9 @@ class SpecLibFlat:
         lib._n_prec = n_prec
         lib._n_frag = n_frag
         lib.device = int(dev)
+        # the columns PeakGroupQuantification passes through (read at quantify time)
+        src = {n: a for n, a, _ in spec} if all(on_dev) else conv
+        lib._passthrough = {n: src[n] for n in _QUANT_PASSTHROUGH}
         return lib
 
     @property
@@ -322,12 +332,15 @@ def _extract_usize(val) -> int:
     return iv
 
 
+_F32_PARAMS = frozenset(_FLOAT_KEYS + ("tolerance_ppm",))
+
+
 def _update_in_order(obj, config: dict, order) -> None:
     """Reads the keys present in ``config`` in the reference's order; the first
     value that does not convert raises, and the keys read before it stay set."""
     for k in order:
         if k in config:
-            conv = _extract_f32 if k in _FLOAT_KEYS else _extract_usize
+            conv = _extract_f32 if k in _F32_PARAMS else _extract_usize
             v = dict(object.__getattribute__(obj, "_v"))
             v[k] = conv(config[k])
             object.__setattr__(obj, "_v", v)
@@ -733,3 +746,163 @@ class PeakGroupScoring:
                                        cols[3].ctypes.data, cols[4].ctypes.data, F.ADS_MEM_HOST,
                                        int(self.verbose), C.byref(out)))
         return CandidateFeatureCollection._from_handle(out.value)
+
+
+# ------------------------------------------------------------------ quantification
+
+class QuantificationParameters:
+    """QuantificationParameters (src/peak_group_quantification/parameters.rs:4-44):
+    tolerance_ppm and top_k_fragments, readable and writable, the defaults of ``new``
+    and ``update(dict)``."""
+
+    __slots__ = ("_v",)
+
+    def __init__(self):
+        p = F.AdsQuantParams()
+        _lib().ads_quant_params_default(C.byref(p))
+        object.__setattr__(self, "_v", {"tolerance_ppm": float(np.float32(p.tolerance_ppm)),
+                                        "top_k_fragments": int(p.top_k_fragments)})
+
+    def __getattr__(self, name):
+        v = object.__getattribute__(self, "_v")
+        if name in v:
+            return v[name]
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        if name not in ("tolerance_ppm", "top_k_fragments"):
+            raise AttributeError(f"'QuantificationParameters' object has no attribute '{name}'")
+        _update_in_order(self, {name: value}, (name,))
+
+    def __delattr__(self, name):
+        raise TypeError("can't delete attribute")
+
+    def update(self, config: dict) -> None:
+        """Sets tolerance_ppm and/or top_k_fragments (parameters.rs:30-37)."""
+        _update_in_order(self, config, ("tolerance_ppm", "top_k_fragments"))
+
+    def _c(self) -> F.AdsQuantParams:
+        p = F.AdsQuantParams()
+        p.tolerance_ppm = self._v["tolerance_ppm"]
+        p.top_k_fragments = min(self._v["top_k_fragments"], 2**63 - 1)
+        return p
+
+    def __repr__(self):
+        return (f"QuantificationParameters(tolerance_ppm={self.tolerance_ppm}, "
+                f"top_k_fragments={self.top_k_fragments})")
+
+
+_QUANT_PRECURSOR_KEYS = ("precursor_idx", "mz_library", "mz", "rt_library", "rt", "naa", "rank",
+                         "rt_observed", "flat_frag_start_idx", "flat_frag_stop_idx")
+_QUANT_FRAGMENT_KEYS = ("mz_library", "mz", "intensity", "cardinality", "charge", "loss_type", "number",
+                        "position", "type", "mz_observed", "correlation_observed", "mass_error_observed",
+                        "precursor_idx", "rank")
+_QUANT_DTYPES = {"precursor_idx": np.uint64, "rank": np.uint64, "flat_frag_start_idx": np.uint64,
+                 "flat_frag_stop_idx": np.uint64, "naa": np.uint8, "cardinality": np.uint8,
+                 "charge": np.uint8, "loss_type": np.uint8, "number": np.uint8, "position": np.uint8,
+                 "type": np.uint8}
+
+
+class SpecLibFlatQuantified:
+    """SpecLibFlatQuantified (src/speclib_flat_quantified/mod.rs:19-210): quantified
+    precursors sorted by precursor_idx, their fragments in candidate order."""
+
+    def __init__(self):
+        self._prec = {k: np.zeros(0, _QUANT_DTYPES.get(k, np.float32)) for k in _QUANT_PRECURSOR_KEYS}
+        self._frag = {k: np.zeros(0, _QUANT_DTYPES.get(k, np.float32)) for k in _QUANT_FRAGMENT_KEYS}
+        self._kernel_ms = 0.0
+
+    @property
+    def num_precursors(self) -> int:
+        return len(self._prec["mz"])
+
+    @property
+    def num_fragments(self) -> int:
+        return len(self._frag["mz"])
+
+    def to_dict_arrays(self) -> tuple:
+        """(precursor dict, fragment dict) (src/speclib_flat_quantified/mod.rs:110-210)."""
+        return ({k: self._prec[k].copy() for k in _QUANT_PRECURSOR_KEYS},
+                {k: self._frag[k].copy() for k in _QUANT_FRAGMENT_KEYS})
+
+    def kernel_ms(self) -> float:
+        """Extension: device time of the quantification kernel in milliseconds."""
+        return self._kernel_ms
+
+
+def _take(src, rows: np.ndarray) -> np.ndarray:
+    """src[rows] for a numpy array or a CUDA tensor, as a numpy array."""
+    if _is_device_tensor(src):
+        import torch
+
+        return src[torch.as_tensor(rows, device=src.device)].cpu().numpy()
+    return np.asarray(src)[rows]
+
+
+class PeakGroupQuantification:
+    """PeakGroupQuantification (src/peak_group_quantification/mod.rs:24-168) on the GPU."""
+
+    def __init__(self, params: QuantificationParameters, *, verbose: bool = True):
+        if not isinstance(params, QuantificationParameters):
+            raise TypeError("argument 'params': expected QuantificationParameters")
+        self.params = params
+        self.verbose = verbose
+
+    def quantify(self, dia_data: DIAData, lib: SpecLibFlat, candidates) -> SpecLibFlatQuantified:
+        """Quantifies every candidate whose precursor is in ``lib``.  ``candidates`` is a
+        CandidateCollection, or (extension) a DeviceCandidates buffer.  The library's
+        pass-through columns are read from the arrays given to SpecLibFlat.from_arrays."""
+        if not isinstance(dia_data, DIAData) or not isinstance(lib, SpecLibFlat) or \
+                not isinstance(candidates, (CandidateCollection, DeviceCandidates)):
+            raise TypeError("quantify(dia_data: DIAData, lib: SpecLibFlat, candidates: CandidateCollection)")
+        if dia_data._h is None or lib._h is None:
+            raise ValueError("DIAData and SpecLibFlat must be built with from_arrays")
+        p = self.params._c()
+        h = C.c_void_p()
+        L = _lib()
+        if isinstance(candidates, DeviceCandidates) or (candidates._h is not None and
+                                                         candidates._arrays is None):
+            F.check(L.ads_quantify(C.byref(p), dia_data._h, lib._h, candidates._h, int(self.verbose),
+                                   C.byref(h)))
+        else:
+            a = candidates._materialize()
+            cols = [np.ascontiguousarray(a[k], np.uint64) for k in
+                    ("precursor_idx", "rank", "cycle_center", "cycle_start", "cycle_stop")]
+            F.check(L.ads_quantify_arrays(C.byref(p), dia_data._h, lib._h, len(cols[0]),
+                                          *[c.ctypes.data for c in cols], F.ADS_MEM_HOST,
+                                          int(self.verbose), C.byref(h)))
+        out = SpecLibFlatQuantified()
+        try:
+            n_p, n_f = C.c_int64(), C.c_int64()
+            F.check(L.ads_quant_sizes(h, C.byref(n_p), C.byref(n_f)))
+            P, NF = n_p.value, n_f.value
+            out._kernel_ms = float(L.ads_quant_kernel_ms(h))
+            u = lambda m: np.empty(max(m, 1), np.uint64)
+            f = lambda m: np.empty(max(m, 1), np.float32)
+            pidx, prow, prank, prt, pfs, pfe = u(P), u(P), u(P), f(P), u(P), u(P)
+            frow, fint, fmzo, fcorr, ferr, fpidx, frank = u(NF), f(NF), f(NF), f(NF), f(NF), u(NF), u(NF)
+            if P:
+                F.check(L.ads_quant_copy_out(h, *[x.ctypes.data for x in (
+                    pidx, prow, prank, prt, pfs, pfe, frow, fint, fmzo, fcorr, ferr, fpidx, frank)]))
+        finally:
+            L.ads_quant_destroy(h)
+        src = lib._passthrough
+        pr, fr = prow[:P].astype(np.int64), frow[:NF].astype(np.int64)
+        out._prec = {"precursor_idx": pidx[:P], "mz_library": _take(src["precursor_mz_library"], pr),
+                     "mz": _take(src["precursor_mz"], pr),
+                     "rt_library": _take(src["precursor_rt_library"], pr),
+                     "rt": _take(src["precursor_rt"], pr), "naa": _take(src["precursor_naa"], pr),
+                     "rank": prank[:P], "rt_observed": prt[:P], "flat_frag_start_idx": pfs[:P],
+                     "flat_frag_stop_idx": pfe[:P]}
+        out._frag = {"mz_library": _take(src["fragment_mz_library"], fr), "mz": _take(src["fragment_mz"], fr),
+                     "intensity": fint[:NF], "cardinality": _take(src["fragment_cardinality"], fr),
+                     "charge": _take(src["fragment_charge"], fr),
+                     "loss_type": _take(src["fragment_loss_type"], fr),
+                     "number": _take(src["fragment_number"], fr),
+                     "position": _take(src["fragment_position"], fr), "type": _take(src["fragment_type"], fr),
+                     "mz_observed": fmzo[:NF], "correlation_observed": fcorr[:NF],
+                     "mass_error_observed": ferr[:NF], "precursor_idx": fpidx[:NF], "rank": frank[:NF]}
+        for d in (out._prec, out._frag):
+            for k, v in d.items():
+                d[k] = np.ascontiguousarray(v, _QUANT_DTYPES.get(k, np.float32))
+        return out

@@ -284,6 +284,7 @@ struct AdsLib {
   float* pmz_p = nullptr;
   float* prt_p = nullptr;
   float* ptol_p = nullptr;     // optional per-precursor RT half-window
+  uint32_t* prow_p = nullptr;  // input row of each sorted precursor
   uint64_t* fstart_p = nullptr;
   uint64_t* fstop_p = nullptr;
   uint8_t* naa_p = nullptr;    // precursor_naa (scoring), sorted like the other precursor arrays

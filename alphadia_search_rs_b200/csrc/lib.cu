@@ -131,6 +131,7 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     lib->pmz_p = c.take<float>(P);
     lib->prt_p = c.take<float>(P);
     lib->ptol_p = lib->has_tol ? c.take<float>(P) : nullptr;
+    lib->prow_p = c.take<uint32_t>(P);
     lib->fstart_p = c.take<uint64_t>(P);
     lib->fstop_p = c.take<uint64_t>(P);
     lib->naa_p = c.take<uint8_t>(P);
@@ -169,7 +170,6 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
       fe_in = q.take<uint64_t>(P);
       naa_in = q.take<uint8_t>(P);
       pos_in = q.take<uint32_t>(P);
-      pos_out = q.take<uint32_t>(P);
       sort_tmp = q.take<char>((int64_t)sort_bytes);
     };
     Carver tsize;
@@ -201,6 +201,7 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     // stable radix sort of (precursor_idx, position): equal keys keep input order
     iota_kernel<<<(int)std::min<int64_t>((P + 255) / 256, 4096), 256, 0, st>>>(P, pos_in);
     ADS_LAUNCH_CHECK();
+    pos_out = lib->prow_p;  // kept: the input row of every sorted precursor
     ADS_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, pidx_in, lib->pidx_p, pos_in,
                                              pos_out, P, 0, 64, st));
     launch_gather(P, pos_out, pmz_in, lib->pmz_p, st);
@@ -210,6 +211,8 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     launch_gather(P, pos_out, naa_in, lib->naa_p, st);
     if (lib->has_tol) launch_gather(P, pos_out, ptol_in, lib->ptol_p, st);
     ADS_LAUNCH_CHECK();
+  } else if (P == 1) {
+    ADS_CUDA(cudaMemsetAsync(lib->prow_p, 0, sizeof(uint32_t), st));
   }
   ADS_CUDA(cudaStreamSynchronize(st));
   *out = lib.release();

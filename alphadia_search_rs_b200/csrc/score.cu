@@ -42,6 +42,24 @@ struct AdsFeatures {
   float kernel_ms = 0.0f;  // CUDA-event time of score_kernel
 };
 
+// Quantified candidates (SpecLibFlatQuantified, src/speclib_flat_quantified/mod.rs:19-64),
+// dense per candidate on the device until ads_quant_copy_out assembles the flat layout.
+struct AdsQuant {
+  int device = 0;
+  int64_t n = 0, n_prec = 0, n_frag = 0;
+  int Fm = 1;
+  ads::DevBuf<char> arena;
+  int* nq_p = nullptr;
+  uint32_t* prow_p = nullptr;
+  float* rt_p = nullptr;
+  uint64_t* pidx_p = nullptr;
+  uint64_t* rank_p = nullptr;
+  uint64_t* frow_p = nullptr;
+  float* fval_p[4] = {nullptr, nullptr, nullptr, nullptr};  // intensity, m/z, correlation, error
+  std::vector<int> nq;
+  float kernel_ms = 0.0f;
+};
+
 namespace ads {
 namespace {
 
@@ -585,6 +603,220 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
   }
 }
 
+// ---------------------------------------------------------------- quantification
+
+// PeakGroupQuantification.quantify per candidate (src/peak_group_quantification/mod.rs:
+// 88-167): outputs of candidate q, dense per candidate (slot j of the first o_nq[q]).
+struct QuantArgs {
+  ScoreArgs s;  // library, run, tolerance, top-k, scratch (o_* and c_score unused)
+  int* o_nq;          // fragments kept (observed intensity > 0); 0 drops the candidate
+  uint32_t* o_prow;   // input row of the precursor
+  float* o_rt;        // rt_observed
+  uint64_t* o_frow;   // [n x Fm] input row of the fragment
+  float* o_int;       // [n x Fm] observed intensity (row sum of the dense XIC)
+  float* o_mzo;       // [n x Fm] observed m/z
+  float* o_corr;      // [n x Fm] correlation with the median of the non-zero profiles
+  float* o_err;       // [n x Fm] mass error (ppm)
+  const uint32_t* l_prow;
+};
+
+// Largest cycle range of the candidates that quantification keeps; error bit 1 when a
+// range ends beyond the run's RT index (the reference would extract zeros past it, or
+// index out of bounds for the centre).
+__global__ void quant_span_kernel(int64_t n, const uint64_t* center, const uint64_t* start,
+                                  const uint64_t* stop, int64_t n_rt, int* span, int* err) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t a = start[q], b = stop[q], c = center[q];
+    if (b <= a || c < a || c >= b) continue;  // dropped (None in the reference)
+    if (b > (uint64_t)n_rt) {
+      atomicOr(err, 1);
+      continue;
+    }
+    const uint64_t d = b - a;
+    atomicMax(span, (int)(d < (uint64_t)INT_MAX ? d : (uint64_t)INT_MAX));
+  }
+}
+
+__global__ void __launch_bounds__(kScoreBlock) quant_kernel(QuantArgs qa) {
+  const ScoreArgs& a = qa.s;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= a.T) return;
+  const Scr s{a.scratch, a.T, t};
+  const int64_t Fm = a.Fm, Cm = a.Cm;
+  // scratch layout (elements), within scratch_words(Fm, Fraw, Cm)
+  const int64_t XIC = 0, MZO = Fm * Cm, NRM = 2 * Fm * Cm, V = 3 * Fm * Cm;
+  const int64_t FMZ = V, FRAW = V + Fm, NZ = V + 2 * Fm, TMP = V + 3 * Fm, MEDF = V + 18 * Fm,
+                KEEP = MEDF + 2 * Cm;
+
+  for (int64_t q = t; q < a.n; q += a.T) {
+    qa.o_nq[q] = 0;
+    const uint64_t cs64 = a.c_start[q], ce64 = a.c_stop[q], center = a.c_center[q];
+    if (ce64 <= cs64 || center < cs64 || center >= ce64) continue;
+    if (ce64 > (uint64_t)a.n_rt || ce64 - cs64 > (uint64_t)Cm) {
+      atomicOr(a.err, 1);
+      continue;
+    }
+    const uint64_t x = a.c_pidx[q];
+    int64_t i = 0;
+    {
+      int64_t size = a.P, base = 0;
+      if (size == 0) continue;
+      while (size > 1) {
+        const int64_t half = size / 2, mid = base + half;
+        base = a.l_pidx[mid] > x ? base : mid;
+        size -= half;
+      }
+      if (a.l_pidx[base] != x) continue;  // get_precursor_by_idx_filtered: None
+      i = base;
+    }
+    // filter_sort_fragments(non-zero, no y1, top-k), as in scoring
+    const int64_t fs = (int64_t)a.l_fs[i], nraw = (int64_t)a.l_fe[i] - fs;
+    if (nraw > a.Fraw) {
+      atomicOr(a.err, 2);
+      continue;
+    }
+    int64_t nk = 0;
+    for (int64_t r = 0; r < nraw; ++r) {
+      const float I = a.l_fint[fs + r];
+      const bool k = I > 0.0f && !(a.l_ftype[fs + r] == 121 && a.l_fnum[fs + r] == 1);
+      s.su(KEEP + r, k ? 1u : 0u);
+      nk += k;
+    }
+    const bool topk = nk > a.top_k;
+    if (topk) {
+      for (int64_t r = 0; r < nraw; ++r) {
+        if (!s.u(KEEP + r)) continue;
+        const float I = a.l_fint[fs + r];
+        int64_t rank = 0;  // ties to the lower position
+        for (int64_t j = 0; j < r; ++j)
+          if (s.u(KEEP + j)) rank += !(a.l_fint[fs + j] < I);
+        for (int64_t j = r + 1; j < nraw; ++j)
+          if (s.u(KEEP + j)) rank += a.l_fint[fs + j] > I;
+        if (rank < a.top_k) s.su(KEEP + r, 2u);
+      }
+    }
+    const uint32_t need = topk ? 2u : 1u;
+    const int64_t F = topk ? a.top_k : nk;
+    for (int64_t r = 0; r < nraw; ++r) {
+      if (s.u(KEEP + r) < need) continue;
+      const float m = a.l_fmz[fs + r];
+      int64_t pos = 0;  // stable: ties keep their library order
+      for (int64_t j = 0; j < r; ++j)
+        if (s.u(KEEP + j) >= need) pos += !(a.l_fmz[fs + j] > m);
+      for (int64_t j = r + 1; j < nraw; ++j)
+        if (s.u(KEEP + j) >= need) pos += a.l_fmz[fs + j] < m;
+      s.sf(FMZ + pos, m);
+      s.su(FRAW + pos, (uint32_t)r);
+    }
+    // DenseXICMZObservation::new over the candidate's cycles
+    const int cs = (int)cs64, ce = (int)ce64;
+    const int64_t C = ce - cs;
+    for (int64_t e = 0; e < F * C; ++e) {
+      s.sf(XIC + e, 0.0f);
+      s.sf(MZO + e, 0.0f);
+    }
+    const float pmz = a.l_pmz[i];
+    for (int w = 0; w < a.n_obs; ++w) {
+      const WinInfo wi = a.win[w];
+      if (!(wi.lo <= pmz && wi.hi >= pmz) || wi.ss_off < 0) continue;  // empty: no peaks
+      const uint32_t* ssw = a.ss + wi.ss_off;
+      const uint16_t* cyw = a.cyc + wi.base;
+      const float* inw = a.inten + wi.base;
+      for (int64_t f = 0; f < F; ++f) {
+        const float mz = s.f(FMZ + f);
+        const float delta = __fmul_rn(__fmul_rn(mz, a.tol), 1e-6f);
+        const uint32_t b0 = grid_lower_bound(a.g, __fsub_rn(mz, delta));
+        const uint32_t b1 = max(b0, grid_upper_bound(a.g, __fadd_rn(mz, delta)));
+        for (uint32_t b = b0; b < b1; ++b) {
+          const float actual = __ldg(a.g.grid + b);
+          const int64_t e0 = ssw[b], e1 = ssw[b + 1];
+          for (int64_t k = e0 + bsearch_u16_rust(cyw + e0, e1 - e0, cs); k < e1; ++k) {
+            const int c = cyw[k];
+            if (c >= ce) break;
+            const int64_t at = f * C + (c - cs);
+            const float v = inw[k];
+            const float xs = __fadd_rn(s.f(XIC + at), v);
+            s.sf(XIC + at, xs);
+            if (v > 0.0f) {
+              const float prev = __fsub_rn(xs, v);
+              if (prev == 0.0f)
+                s.sf(MZO + at, actual);
+              else
+                s.sf(MZO + at, __fdiv_rn(__fadd_rn(__fmul_rn(s.f(MZO + at), prev),
+                                                   __fmul_rn(actual, v)),
+                                         xs));
+            }
+          }
+        }
+      }
+    }
+    // normalize_profiles(xic, 1) and the rows that stay non-zero
+    {
+      const int64_t center_c = C / 2;
+      const int64_t c0 = center_c > 1 ? center_c - 1 : 0;
+      const int64_t c1 = center_c + 2 < C ? center_c + 2 : C;
+      for (int64_t f = 0; f < F; ++f) {
+        float sum = 0.0f;
+        int64_t count = 0;
+        for (int64_t j = c0; j < c1; ++j) {
+          sum = __fadd_rn(sum, s.f(XIC + f * C + j));
+          ++count;
+        }
+        const float mean = count > 0 ? __fdiv_rn(sum, (float)count) : 0.0f;
+        uint32_t nz = 0;
+        for (int64_t j = 0; j < C; ++j) {
+          const float v = mean > 0.0f ? __fdiv_rn(s.f(XIC + f * C + j), mean) : 0.0f;
+          s.sf(NRM + f * C + j, v);
+          nz |= v != 0.0f;
+        }
+        s.su(NZ + f, nz);
+      }
+    }
+    // filter_non_zero + median_axis_0 (zeros when no row is non-zero)
+    for (int64_t j = 0; j < C; ++j) {
+      int64_t R = 0;
+      for (int64_t f = 0; f < F; ++f)
+        if (s.u(NZ + f)) s.sf(TMP + R++, s.f(NRM + f * C + j));
+      float med = 0.0f;
+      if (R > 0) {
+        sort_floats(s, TMP, R);
+        med = R % 2 == 0 ? __fdiv_rn(__fadd_rn(s.f(TMP + R / 2 - 1), s.f(TMP + R / 2)), 2.0f)
+                         : s.f(TMP + R / 2);
+      }
+      s.sf(MEDF + j, med);
+    }
+    // per fragment: observed m/z and mass error, correlation, observed intensity; the
+    // fragments with a positive observed intensity are kept in m/z order
+    int nq = 0;
+    for (int64_t f = 0; f < F; ++f) {
+      const float obs = ndarray_sum(s, XIC + f * C, C);
+      if (!(obs > 0.0f)) continue;  // PrecursorQuantified::filter_fragments_by_intensity(0.0)
+      float ws = 0.0f, wsum = 0.0f;
+      for (int64_t j = 0; j < C; ++j) {
+        const float w = s.f(XIC + f * C + j);
+        if (w > 0.0f) {
+          ws = __fadd_rn(ws, __fmul_rn(s.f(MZO + f * C + j), w));
+          wsum = __fadd_rn(wsum, w);
+        }
+      }
+      const float o = wsum > 0.0f ? __fdiv_rn(ws, wsum) : 0.0f;
+      const float lib = s.f(FMZ + f);
+      const int64_t slot = q * Fm + nq;
+      qa.o_frow[slot] = (uint64_t)fs + s.u(FRAW + f);
+      qa.o_int[slot] = obs;
+      qa.o_mzo[slot] = o;
+      qa.o_err[slot] = o > 0.0f ? __fmul_rn(__fdiv_rn(__fsub_rn(o, lib), lib), 1e6f) : 0.0f;
+      // calculate_correlation_safe(profile, median) is symmetric in its arguments
+      qa.o_corr[slot] = correlation_safe(s, MEDF, NRM + f * C, C);
+      ++nq;
+    }
+    qa.o_nq[q] = nq;
+    qa.o_prow[q] = qa.l_prow[i];
+    qa.o_rt[q] = a.rt[center];
+  }
+}
+
 // The library's IDF histogram, built once per library on the device.
 int ensure_idf(AdsLib* l, const GridView& g, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(l->mu);
@@ -710,6 +942,150 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
     fflush(stdout);
   }
   *out = f.release();
+  return ADS_OK;
+}
+
+int quant_device(const AdsQuantParams* p, const AdsDia* d, AdsLib* l, int64_t n,
+                 const uint64_t* pidx, const uint64_t* rank, const uint64_t* center,
+                 const uint64_t* start, const uint64_t* stop, int verbose, AdsQuant** out) {
+  if (!(p->tolerance_ppm == p->tolerance_ppm))
+    return fail(ADS_ERR_INVALID_ARGUMENT, "tolerance_ppm is NaN");
+  if (p->top_k_fragments < 0) return fail(ADS_ERR_INVALID_ARGUMENT, "top_k_fragments < 0");
+  cudaStream_t st = cudaStreamPerThread;
+  GridView g;
+  ADS_TRY(device_grid(d->device, &g));
+  auto r = std::make_unique<AdsQuant>();
+  r->device = d->device;
+  r->n = n;
+  DevBuf<int> tmp;
+  ADS_TRY(tmp.alloc(2));
+  ADS_CUDA(cudaMemsetAsync(tmp.p, 0, 8, st));
+  int64_t c_max = 0;
+  if (n > 0) {
+    quant_span_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(
+        n, center, start, stop, (int64_t)d->rt.size(), tmp.p, tmp.p + 1);
+    ADS_LAUNCH_CHECK();
+    int h[2];
+    ADS_CUDA(cudaMemcpyAsync(h, tmp.p, 8, cudaMemcpyDeviceToHost, st));
+    ADS_CUDA(cudaStreamSynchronize(st));
+    if (h[1])
+      return fail(ADS_ERR_INVALID_ARGUMENT, "candidate cycle range ends beyond the run's RT index");
+    c_max = h[0];
+  }
+  const int Fm = (int)std::max<int64_t>(1, std::min<int64_t>(p->top_k_fragments, l->max_frag));
+  const int Fraw = (int)std::max<int64_t>(1, l->max_frag);
+  const int Cm = (int)std::max<int64_t>(1, c_max);
+  r->Fm = Fm;
+  const size_t n1 = (size_t)std::max<int64_t>(n, 1), ns = n1 * (size_t)Fm;
+  auto rnd = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t b_nq = rnd(n1 * 4), b_prow = rnd(n1 * 4), b_rt = rnd(n1 * 4), b_pid = rnd(n1 * 8),
+               b_rank = rnd(n1 * 8), b_frow = rnd(ns * 8), b_f = rnd(ns * 4);
+  ADS_TRY(r->arena.alloc(b_nq + b_prow + b_rt + b_pid + b_rank + b_frow + 4 * b_f));
+  char* base = r->arena.p;
+  r->nq_p = reinterpret_cast<int*>(base);
+  base += b_nq;
+  r->prow_p = reinterpret_cast<uint32_t*>(base);
+  base += b_prow;
+  r->rt_p = reinterpret_cast<float*>(base);
+  base += b_rt;
+  r->pidx_p = reinterpret_cast<uint64_t*>(base);
+  base += b_pid;
+  r->rank_p = reinterpret_cast<uint64_t*>(base);
+  base += b_rank;
+  r->frow_p = reinterpret_cast<uint64_t*>(base);
+  base += b_frow;
+  for (int k = 0; k < 4; ++k) {
+    r->fval_p[k] = reinterpret_cast<float*>(base);
+    base += b_f;
+  }
+  if (n > 0) {
+    ADS_CUDA(cudaMemcpyAsync(r->pidx_p, pidx, (size_t)n * 8, cudaMemcpyDeviceToDevice, st));
+    ADS_CUDA(cudaMemcpyAsync(r->rank_p, rank, (size_t)n * 8, cudaMemcpyDeviceToDevice, st));
+    const int64_t words = scratch_words(Fm, Fraw, Cm);
+    int n_sm = 0;
+    ADS_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, d->device));
+    int64_t T = std::min<int64_t>(n, (int64_t)n_sm * 16 * kScoreBlock);
+    T = std::max<int64_t>(1, std::min<int64_t>(T, ((int64_t)1 << 28) / words));  // <= 1 GiB
+    DevBuf<uint32_t> scratch;
+    ADS_TRY(scratch.alloc((size_t)(T * words)));
+    QuantArgs qa;
+    std::memset(&qa, 0, sizeof(qa));
+    ScoreArgs& a = qa.s;
+    a.n = n;
+    a.c_pidx = pidx;
+    a.c_rank = rank;
+    a.c_center = center;
+    a.c_start = start;
+    a.c_stop = stop;
+    a.P = l->n_prec;
+    a.l_pidx = l->pidx_p;
+    a.l_pmz = l->pmz_p;
+    a.l_prt = l->prt_p;
+    a.l_fs = l->fstart_p;
+    a.l_fe = l->fstop_p;
+    a.l_fmz = l->fmz_p;
+    a.l_fint = l->fint_p;
+    a.l_fnum = l->fnum_p;
+    a.l_ftype = l->ftype_p;
+    a.win = d->win_dev.p;
+    a.n_obs = (int)d->n_obs;
+    a.ss = d->slice_starts.p;
+    a.cyc = d->cycles.p;
+    a.inten = d->intens.p;
+    a.rt = d->rt_dev.p;
+    a.n_rt = (int64_t)d->rt.size();
+    a.g = g;
+    a.tol = p->tolerance_ppm;
+    a.top_k = p->top_k_fragments;
+    a.Fm = Fm;
+    a.Fraw = Fraw;
+    a.Cm = Cm;
+    a.scratch = scratch.p;
+    a.T = T;
+    a.err = tmp.p + 1;
+    qa.o_nq = r->nq_p;
+    qa.o_prow = r->prow_p;
+    qa.o_rt = r->rt_p;
+    qa.o_frow = r->frow_p;
+    qa.o_int = r->fval_p[0];
+    qa.o_mzo = r->fval_p[1];
+    qa.o_corr = r->fval_p[2];
+    qa.o_err = r->fval_p[3];
+    qa.l_prow = l->prow_p;
+    struct Events {
+      cudaEvent_t a = nullptr, b = nullptr;
+      ~Events() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+      }
+    } ev;
+    ADS_CUDA(cudaEventCreate(&ev.a));
+    ADS_CUDA(cudaEventCreate(&ev.b));
+    ADS_CUDA(cudaEventRecord(ev.a, st));
+    quant_kernel<<<(int)((T + kScoreBlock - 1) / kScoreBlock), kScoreBlock, 0, st>>>(qa);
+    ADS_LAUNCH_CHECK();
+    ADS_CUDA(cudaEventRecord(ev.b, st));
+    r->nq.resize((size_t)n);
+    ADS_CUDA(cudaMemcpyAsync(r->nq.data(), r->nq_p, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    int herr = 0;
+    ADS_CUDA(cudaMemcpyAsync(&herr, tmp.p + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ADS_CUDA(cudaStreamSynchronize(st));
+    if (herr & 1)
+      return fail(ADS_ERR_INVALID_ARGUMENT, "candidate cycle range ends beyond the run's RT index");
+    if (herr & 2) return fail(ADS_ERR_INTERNAL, "fragment count above the scratch plan");
+    ADS_CUDA(cudaEventElapsedTime(&r->kernel_ms, ev.a, ev.b));
+    for (int v : r->nq) {
+      r->n_frag += v;
+      r->n_prec += v > 0;
+    }
+  }
+  if (verbose) {
+    // src/peak_group_quantification/mod.rs:73-78 (the kernel's device time)
+    printf("Peak group quantification completed in %.2fs for %lld precursors\n",
+           (double)r->kernel_ms * 1e-3, (long long)r->n_prec);
+    fflush(stdout);
+  }
+  *out = r.release();
   return ADS_OK;
 }
 
@@ -848,6 +1224,136 @@ int ads_features_destroy(AdsFeatures* f) {
 int ads_feature_names(const char** names, int cap) {
   for (int k = 0; k < kFeatures && k < cap; ++k) names[k] = kFeatureNames[k];
   return kFeatures;
+}
+
+void ads_quant_params_default(AdsQuantParams* p) {
+  if (!p) return;
+  // QuantificationParameters::new (src/peak_group_quantification/parameters.rs:19-28)
+  p->tolerance_ppm = 7.0f;
+  p->top_k_fragments = 10000;
+}
+
+int ads_quantify(const AdsQuantParams* params, const AdsDia* dia, AdsLib* lib, AdsCandidates* cand,
+                 int verbose, AdsQuant** out) {
+  return guarded([&] {
+    if (!params || !dia || !lib || !cand || !out) return fail(ADS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (dia->device != lib->device || cand->device != lib->device)
+      return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
+    const int64_t n = ads_candidates_size(cand);  // waits for the search that fills them
+    if (n < 0) return fail(ADS_ERR_INTERNAL, ads_last_error());
+    DeviceGuard dg(dia->device);
+    return quant_device(params, dia, lib, n, cand->pidx_p, cand->rank_p, cand->center_p,
+                        cand->start_p, cand->stop_p, verbose, out);
+  });
+}
+
+int ads_quantify_arrays(const AdsQuantParams* params, const AdsDia* dia, AdsLib* lib, int64_t n,
+                        const uint64_t* precursor_idx, const uint64_t* rank,
+                        const uint64_t* cycle_center, const uint64_t* cycle_start,
+                        const uint64_t* cycle_stop, int location, int verbose, AdsQuant** out) {
+  return guarded([&] {
+    if (!params || !dia || !lib || !out) return fail(ADS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (n < 0) return fail(ADS_ERR_INVALID_ARGUMENT, "negative candidate count");
+    if (location != ADS_MEM_HOST && location != ADS_MEM_DEVICE)
+      return fail(ADS_ERR_INVALID_ARGUMENT, "location must be ADS_MEM_HOST or ADS_MEM_DEVICE");
+    if (n > 0 && (!precursor_idx || !rank || !cycle_center || !cycle_start || !cycle_stop))
+      return fail(ADS_ERR_INVALID_ARGUMENT, "null array pointer");
+    if (dia->device != lib->device) return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
+    DeviceGuard dg(dia->device);
+    cudaStream_t st = cudaStreamPerThread;
+    const size_t n1 = (size_t)std::max<int64_t>(n, 1);
+    DevBuf<uint64_t> cols;
+    ADS_TRY(cols.alloc(5 * n1));
+    const cudaMemcpyKind kind = location == ADS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (n > 0) {
+      const uint64_t* src[5] = {precursor_idx, rank, cycle_center, cycle_start, cycle_stop};
+      for (int k = 0; k < 5; ++k)
+        ADS_CUDA(cudaMemcpyAsync(cols.p + k * n1, src[k], (size_t)n * 8, kind, st));
+    }
+    return quant_device(params, dia, lib, n, cols.p, cols.p + n1, cols.p + 2 * n1, cols.p + 3 * n1,
+                        cols.p + 4 * n1, verbose, out);
+  });
+}
+
+int ads_quant_sizes(const AdsQuant* q, int64_t* n_precursors, int64_t* n_fragments) {
+  if (!q) return fail(ADS_ERR_INVALID_ARGUMENT, "null handle");
+  if (n_precursors) *n_precursors = q->n_prec;
+  if (n_fragments) *n_fragments = q->n_frag;
+  return ADS_OK;
+}
+
+float ads_quant_kernel_ms(const AdsQuant* q) { return q ? q->kernel_ms : -1.0f; }
+
+int ads_quant_copy_out(const AdsQuant* q, uint64_t* precursor_idx, uint64_t* precursor_row,
+                       uint64_t* rank, float* rt_observed, uint64_t* flat_frag_start_idx,
+                       uint64_t* flat_frag_stop_idx, uint64_t* fragment_row, float* intensity,
+                       float* mz_observed, float* correlation_observed, float* mass_error_observed,
+                       uint64_t* fragment_precursor_idx, uint64_t* fragment_rank) {
+  return guarded([&] {
+    if (!q) return fail(ADS_ERR_INVALID_ARGUMENT, "null handle");
+    if (q->n_prec == 0) return ADS_OK;
+    DeviceGuard dg(q->device);
+    const size_t n = (size_t)q->n, Fm = (size_t)q->Fm;
+    std::vector<uint32_t> prow(n);
+    std::vector<float> rt(n);
+    std::vector<uint64_t> pid(n), rk(n), frow(n * Fm);
+    std::vector<float> fv[4];
+    ADS_CUDA(cudaMemcpy(prow.data(), q->prow_p, n * 4, cudaMemcpyDeviceToHost));
+    ADS_CUDA(cudaMemcpy(rt.data(), q->rt_p, n * 4, cudaMemcpyDeviceToHost));
+    ADS_CUDA(cudaMemcpy(pid.data(), q->pidx_p, n * 8, cudaMemcpyDeviceToHost));
+    ADS_CUDA(cudaMemcpy(rk.data(), q->rank_p, n * 8, cudaMemcpyDeviceToHost));
+    ADS_CUDA(cudaMemcpy(frow.data(), q->frow_p, n * Fm * 8, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 4; ++k) {
+      fv[k].resize(n * Fm);
+      ADS_CUDA(cudaMemcpy(fv[k].data(), q->fval_p[k], n * Fm * 4, cudaMemcpyDeviceToHost));
+    }
+    float* fout[4] = {intensity, mz_observed, correlation_observed, mass_error_observed};
+    // SpecLibFlatQuantified::from_precursor_quantified_vec (src/speclib_flat_quantified/
+    // mod.rs:212-333): fragments in candidate order, precursors stably sorted by idx
+    std::vector<size_t> kept;
+    std::vector<uint64_t> fs, fe;
+    uint64_t o = 0;
+    for (size_t c = 0; c < n; ++c) {
+      const int k = q->nq[c];
+      if (k <= 0) continue;
+      kept.push_back(c);
+      fs.push_back(o);
+      for (int j = 0; j < k; ++j, ++o) {
+        const size_t slot = c * Fm + (size_t)j;
+        if (fragment_row) fragment_row[o] = frow[slot];
+        for (int v = 0; v < 4; ++v)
+          if (fout[v]) fout[v][o] = fv[v][slot];
+        if (fragment_precursor_idx) fragment_precursor_idx[o] = pid[c];
+        if (fragment_rank) fragment_rank[o] = rk[c];
+      }
+      fe.push_back(o);
+    }
+    std::vector<size_t> ord(kept.size());
+    for (size_t k = 0; k < ord.size(); ++k) ord[k] = k;
+    std::stable_sort(ord.begin(), ord.end(),
+                     [&](size_t x, size_t y) { return pid[kept[x]] < pid[kept[y]]; });
+    for (size_t j = 0; j < ord.size(); ++j) {
+      const size_t k = ord[j], c = kept[k];
+      if (precursor_idx) precursor_idx[j] = pid[c];
+      if (precursor_row) precursor_row[j] = prow[c];
+      if (rank) rank[j] = rk[c];
+      if (rt_observed) rt_observed[j] = rt[c];
+      if (flat_frag_start_idx) flat_frag_start_idx[j] = fs[k];
+      if (flat_frag_stop_idx) flat_frag_stop_idx[j] = fe[k];
+    }
+    return ADS_OK;
+  });
+}
+
+int ads_quant_destroy(AdsQuant* q) {
+  return guarded([&] {
+    if (!q) return ADS_OK;
+    DeviceGuard dg(q->device);
+    delete q;
+    return ADS_OK;
+  });
 }
 
 }  // extern "C"

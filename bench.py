@@ -51,7 +51,7 @@ def parse():
                     help="MS2 windows in the CPU-baseline sample (0: about 72 M peaks' worth)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-scoring", action="store_true",
-                    help="skip the PeakGroupScoring figures added to the JSON line")
+                    help="skip the scoring and quantification figures added to the JSON line")
     ap.add_argument("--warps-per-block", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--cycles-per-lane", type=int, default=0)
@@ -344,6 +344,67 @@ def scoring_figures(ads, dia, slib, cand, out_np, steps: int = 3) -> dict:
             "timing": f"median of {steps} calls after one warm-up"}
 
 
+def quant_figures(ads, dia, slib, cand, steps: int = 3) -> dict:
+    """PeakGroupQuantification.quantify of the search's candidates: the kernel's device
+    time and the whole call (kernel, copy-out, assembly of SpecLibFlatQuantified with
+    its pass-through columns)."""
+    import torch
+
+    q = ads.PeakGroupQuantification(ads.QuantificationParameters(), verbose=False)
+    q.quantify(dia, slib, cand)  # warm-up
+    k_ms, call_s = [], []
+    r = None
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = q.quantify(dia, slib, cand)
+        call_s.append(time.perf_counter() - t0)
+        k_ms.append(r.kernel_ms())
+    n = cand.size()
+    kms = statistics.median(k_ms)
+    return {"metric": "candidates quantified per second (PeakGroupQuantification.quantify)",
+            "value": n / (kms / 1e3), "unit": "candidates/s", "candidates": int(n),
+            "precursors_out": int(r.num_precursors), "fragments_out": int(r.num_fragments),
+            "kernel_ms": kms, "call_ms": 1e3 * statistics.median(call_s),
+            "call_value": n / statistics.median(call_s),
+            "timing": f"median of {steps} calls after one warm-up; the call includes the "
+                      f"device-to-host copy and the SpecLibFlatQuantified assembly"}
+
+
+def quant_cpu_and_parity(ads, oracle, dsub, lsub, od, ol, la: dict, res: dict, n_threads: int,
+                         steps: int = 3):
+    """The oracle's PeakGroupQuantification on the CPU sample's candidates (timed), and
+    the device's result for the same candidates against it, every column bit for bit."""
+    cols = {k: res[k] for k in ("precursor_idx", "rank", "score", "cycle_center", "cycle_start",
+                                "cycle_stop")}
+    oracle.quantify(od, ol, cols, la, n_threads=n_threads)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ref = oracle.quantify(od, ol, cols, la, n_threads=n_threads)
+        ts.append(time.perf_counter() - t0)
+    nc = len(cols["rank"])
+    cpu = {"value": nc / statistics.mean(ts), "unit": "candidates/s", "cores": n_threads,
+           "kind": "port", "sample": f"the {nc} candidates of the search CPU sample, mean of "
+                                     f"{steps} timed calls"}
+    z = np.zeros(nc, np.uint64)
+    cc = ads.CandidateCollection.from_arrays(cols["precursor_idx"], cols["rank"], cols["score"], z, z, z,
+                                             cols["cycle_center"], cols["cycle_start"], cols["cycle_stop"])
+    gp, gf = ads.PeakGroupQuantification(ads.QuantificationParameters(),
+                                         verbose=False).quantify(dsub, lsub, cc).to_dict_arrays()
+    diff = []
+    for part, g, r in (("precursor", gp, ref[0]), ("fragment", gf, ref[1])):
+        for k in r:
+            a, b = np.asarray(g[k]), np.asarray(r[k])
+            same = len(a) == len(b) and (np.array_equal(a.view(np.uint32), b.view(np.uint32))
+                                         if a.dtype == np.float32 else np.array_equal(a, b))
+            if not same:
+                diff.append(f"{part}.{k}")
+    parity = {"candidates": int(nc), "precursors": int(len(ref[0]["precursor_idx"])),
+              "fragments": int(len(ref[1]["mz"])), "bit_identical": not diff, "columns_differing": diff}
+    return cpu, parity
+
+
 def scoring_cpu_and_parity(ads, oracle, host: dict, sub: dict, od, ol, res: dict, n_threads: int,
                            local_rank: int, steps: int = 3):
     """The oracle's PeakGroupScoring on the CPU sample's candidates (timed), and the
@@ -378,8 +439,8 @@ def scoring_cpu_and_parity(ads, oracle, host: dict, sub: dict, od, ol, res: dict
             if not same_rows or not np.array_equal(got[k].view(np.uint32), ref[k].view(np.uint32))]
     parity = {"candidates": int(nc), "rows_identical": bool(same_rows),
               "features_bit_identical": len(diff) == 0, "features_differing": diff}
-    del dsub, lsub, cc
-    return cpu, parity
+    del cc
+    return cpu, parity, (dsub, lsub, la)
 
 
 def oracle_setup(host: dict, sub: dict, n_threads: int):
@@ -666,9 +727,10 @@ def run_ours(args, rank, world, local_rank):
     #      parity spot check of the GPU result for the same precursors
     cpu = None
     parity = None
-    scoring = None
+    scoring = quant = None
     if world == 1 and not args.no_scoring:
         scoring = scoring_figures(ads, dia, slib, cand, out_np)
+        quant = quant_figures(ads, dia, slib, cand)
     if world == 1 and not args.no_cpu_baseline:
         import oracle
 
@@ -695,8 +757,11 @@ def run_ours(args, rank, world, local_rank):
                   "indices_identical": all(same.values()) and int(mask.sum()) == len(res["rank"]),
                   "max_score_rel_err_vs_glibc_logf": rel}
         if scoring is not None:
-            scoring["cpu_baseline"], scoring["parity_sample"] = scoring_cpu_and_parity(
-                ads, oracle, host, sub, od, ol, res, n, local_rank)
+            scoring["cpu_baseline"], scoring["parity_sample"], (dsub, lsub, la_sub) = \
+                scoring_cpu_and_parity(ads, oracle, host, sub, od, ol, res, n, local_rank)
+            quant["cpu_baseline"], quant["parity_sample"] = quant_cpu_and_parity(
+                ads, oracle, dsub, lsub, od, ol, la_sub, res, n)
+            del dsub, lsub
         if precision == "bf16":
             # BF16 storage is compared with the FP64 oracle: top-K cycle agreement and
             # relative score error (against max(|s64|, 1e-3 * the precursor's largest |s64|))
@@ -737,6 +802,7 @@ def run_ours(args, rank, world, local_rank):
         "cpu_baseline": cpu,
         "parity_sample": parity,
         "scoring": scoring,
+        "quantification": quant,
         "clocks": clk.summary(),
         "setup_s": {"generate": t_gen, "dia_build": t_dia, "lib_build": t_lib},
         "counters": stats,

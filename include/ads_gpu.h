@@ -318,6 +318,50 @@ int ads_features_destroy(AdsFeatures* features);
 /* Writes up to cap feature names; returns their number (41). */
 int ads_feature_names(const char** names, int cap);
 
+/* ---- PeakGroupQuantification (src/peak_group_quantification/mod.rs:49-168) ---- */
+
+/* QuantificationParameters (src/peak_group_quantification/parameters.rs:4-37). */
+typedef struct AdsQuantParams {
+  float tolerance_ppm;     /* default 7.0 */
+  int64_t top_k_fragments; /* default 10000 */
+} AdsQuantParams;
+void ads_quant_params_default(AdsQuantParams* p);
+
+/* SpecLibFlatQuantified (src/speclib_flat_quantified/mod.rs:19-64), device resident
+ * until copied out. */
+typedef struct AdsQuant AdsQuant;
+/* PeakGroupQuantification.quantify of the candidates a search left on the device: per
+ * candidate its precursor's fragments (filtered, top-k, m/z order) with the dense XIC's
+ * row sums as observed intensity, the intensity-weighted observed m/z and its ppm error,
+ * and the correlation with the median of the non-zero normalised profiles; fragments
+ * with an observed intensity of 0 are dropped, and so is a candidate left without any
+ * (as are unknown precursors, empty cycle ranges and centres outside them).  A range
+ * that ends beyond the run's RT index is an ADS_ERR_INVALID_ARGUMENT. */
+int ads_quantify(const AdsQuantParams* params, const AdsDia* dia, AdsLib* lib, AdsCandidates* cand,
+                 int verbose, AdsQuant** out);
+/* The same for candidate columns given as arrays, host or device memory. */
+int ads_quantify_arrays(const AdsQuantParams* params, const AdsDia* dia, AdsLib* lib, int64_t n,
+                        const uint64_t* precursor_idx, const uint64_t* rank,
+                        const uint64_t* cycle_center, const uint64_t* cycle_start,
+                        const uint64_t* cycle_stop, int location, int verbose, AdsQuant** out);
+int ads_quant_sizes(const AdsQuant* quant, int64_t* n_precursors, int64_t* n_fragments);
+/* Device time of the quantification kernel in ms (an addition). */
+float ads_quant_kernel_ms(const AdsQuant* quant);
+/* Copies the SpecLibFlatQuantified layout into host arrays (any may be NULL): per
+ * precursor (n_precursors, sorted by precursor_idx, ties in candidate order)
+ * precursor_idx, the precursor's row in the arrays given to ads_lib_create, rank,
+ * rt_observed and its [start, stop) range of fragments; per fragment (n_fragments, in
+ * candidate order) its row in the library's fragment arrays, observed intensity,
+ * observed m/z, correlation, mass error, precursor_idx and rank.  The library's
+ * pass-through columns (m/z, RT, naa, fragment annotations) are the caller's arrays at
+ * those rows (src/speclib_flat_quantified/mod.rs:110-210). */
+int ads_quant_copy_out(const AdsQuant* quant, uint64_t* precursor_idx, uint64_t* precursor_row,
+                       uint64_t* rank, float* rt_observed, uint64_t* flat_frag_start_idx,
+                       uint64_t* flat_frag_stop_idx, uint64_t* fragment_row, float* intensity,
+                       float* mz_observed, float* correlation_observed, float* mass_error_observed,
+                       uint64_t* fragment_precursor_idx, uint64_t* fragment_rank);
+int ads_quant_destroy(AdsQuant* quant);
+
 #ifdef __cplusplus
 }
 #endif

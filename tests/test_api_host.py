@@ -96,6 +96,39 @@ def test_scoring_argument_types():
         ads.PeakGroupScoring({"mass_tolerance": 7.0})
 
 
+def test_quantification_parameters():  # src/peak_group_quantification/tests.rs:15-90
+    p = ads.QuantificationParameters()
+    assert p.tolerance_ppm == 7.0 and p.top_k_fragments == 10000
+    p.tolerance_ppm = 12.0
+    p.top_k_fragments = 50
+    assert (p.tolerance_ppm, p.top_k_fragments) == (12.0, 50)
+    p.update({"tolerance_ppm": 15.0})
+    assert (p.tolerance_ppm, p.top_k_fragments) == (15.0, 50)
+    p.update({"tolerance_ppm": 20.0, "top_k_fragments": 200})
+    assert (p.tolerance_ppm, p.top_k_fragments) == (20.0, 200)
+    p.update({})
+    assert (p.tolerance_ppm, p.top_k_fragments) == (20.0, 200)
+    with pytest.raises(TypeError):
+        p.top_k_fragments = 1.5
+    with pytest.raises(OverflowError):
+        p.update({"top_k_fragments": -1})
+    with pytest.raises(AttributeError):
+        p.other = 1
+
+
+def test_empty_quantified_library():  # src/speclib_flat_quantified/tests.rs:29-41
+    q = ads.SpecLibFlatQuantified()
+    assert q.num_precursors == 0 and q.num_fragments == 0
+    prec, frag = q.to_dict_arrays()
+    assert list(prec) == ["precursor_idx", "mz_library", "mz", "rt_library", "rt", "naa", "rank",
+                          "rt_observed", "flat_frag_start_idx", "flat_frag_stop_idx"]
+    assert list(frag) == ["mz_library", "mz", "intensity", "cardinality", "charge", "loss_type",
+                          "number", "position", "type", "mz_observed", "correlation_observed",
+                          "mass_error_observed", "precursor_idx", "rank"]
+    with pytest.raises(TypeError):
+        ads.PeakGroupQuantification(ads.QuantificationParameters(), verbose=False).quantify(None, None, None)
+
+
 def test_candidate_collection_roundtrip():  # src/candidate/tests.rs:104-156
     cols = dict(precursor_idxs=[1, 2], ranks=[10, 20], scores=[0.1, 0.2], scan_center=[11, 21],
                 scan_start=[12, 22], scan_stop=[13, 23], cycle_center=[14, 24], cycle_start=[15, 25],
