@@ -830,13 +830,23 @@ class SpecLibFlatQuantified:
         return self._kernel_ms
 
 
-def _take(src, rows: np.ndarray) -> np.ndarray:
-    """src[rows] for a numpy array or a CUDA tensor, as a numpy array."""
-    if _is_device_tensor(src):
-        import torch
+class _Rows:
+    """Row indices for the pass-through gathers, moved to a CUDA device at most once."""
 
-        return src[torch.as_tensor(rows, device=src.device)].cpu().numpy()
-    return np.asarray(src)[rows]
+    def __init__(self, rows: np.ndarray):
+        self.rows = rows
+        self._dev = {}
+
+    def take(self, src) -> np.ndarray:
+        """src[rows] for a numpy array or a CUDA tensor, as a numpy array."""
+        if _is_device_tensor(src):
+            import torch
+
+            key = src.device
+            if key not in self._dev:
+                self._dev[key] = torch.from_numpy(self.rows).to(src.device, non_blocking=False)
+            return src.index_select(0, self._dev[key]).cpu().numpy()
+        return np.asarray(src)[self.rows]
 
 
 class PeakGroupQuantification:
@@ -887,19 +897,19 @@ class PeakGroupQuantification:
         finally:
             L.ads_quant_destroy(h)
         src = lib._passthrough
-        pr, fr = prow[:P].astype(np.int64), frow[:NF].astype(np.int64)
-        out._prec = {"precursor_idx": pidx[:P], "mz_library": _take(src["precursor_mz_library"], pr),
-                     "mz": _take(src["precursor_mz"], pr),
-                     "rt_library": _take(src["precursor_rt_library"], pr),
-                     "rt": _take(src["precursor_rt"], pr), "naa": _take(src["precursor_naa"], pr),
+        pr, fr = _Rows(prow[:P].view(np.int64)), _Rows(frow[:NF].view(np.int64))
+        out._prec = {"precursor_idx": pidx[:P], "mz_library": pr.take(src["precursor_mz_library"]),
+                     "mz": pr.take(src["precursor_mz"]),
+                     "rt_library": pr.take(src["precursor_rt_library"]),
+                     "rt": pr.take(src["precursor_rt"]), "naa": pr.take(src["precursor_naa"]),
                      "rank": prank[:P], "rt_observed": prt[:P], "flat_frag_start_idx": pfs[:P],
                      "flat_frag_stop_idx": pfe[:P]}
-        out._frag = {"mz_library": _take(src["fragment_mz_library"], fr), "mz": _take(src["fragment_mz"], fr),
-                     "intensity": fint[:NF], "cardinality": _take(src["fragment_cardinality"], fr),
-                     "charge": _take(src["fragment_charge"], fr),
-                     "loss_type": _take(src["fragment_loss_type"], fr),
-                     "number": _take(src["fragment_number"], fr),
-                     "position": _take(src["fragment_position"], fr), "type": _take(src["fragment_type"], fr),
+        out._frag = {"mz_library": fr.take(src["fragment_mz_library"]), "mz": fr.take(src["fragment_mz"]),
+                     "intensity": fint[:NF], "cardinality": fr.take(src["fragment_cardinality"]),
+                     "charge": fr.take(src["fragment_charge"]),
+                     "loss_type": fr.take(src["fragment_loss_type"]),
+                     "number": fr.take(src["fragment_number"]),
+                     "position": fr.take(src["fragment_position"]), "type": fr.take(src["fragment_type"]),
                      "mz_observed": fmzo[:NF], "correlation_observed": fcorr[:NF],
                      "mass_error_observed": ferr[:NF], "precursor_idx": fpidx[:NF], "rank": frank[:NF]}
         for d in (out._prec, out._frag):

@@ -18,6 +18,8 @@
 // A thread's matrices (F x C dense XIC, m/z and normalised profiles) and vectors
 // live in a global scratch interleaved across threads (element e of thread t at
 // e * T + t), so threads working on the same element read consecutive words.
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -58,6 +60,12 @@ struct AdsQuant {
   float* fval_p[4] = {nullptr, nullptr, nullptr, nullptr};  // intensity, m/z, correlation, error
   std::vector<int> nq;
   float kernel_ms = 0.0f;
+  // the flat SpecLibFlatQuantified layout, assembled on the device
+  ads::DevBuf<char> flat;
+  uint64_t *p_idx = nullptr, *p_row = nullptr, *p_rank = nullptr, *p_fs = nullptr, *p_fe = nullptr;
+  float* p_rt = nullptr;
+  uint64_t *f_row = nullptr, *f_pidx = nullptr, *f_rank = nullptr;
+  float* f_val[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace ads {
@@ -817,6 +825,140 @@ __global__ void __launch_bounds__(kScoreBlock) quant_kernel(QuantArgs qa) {
   }
 }
 
+// SpecLibFlatQuantified::from_precursor_quantified_vec (src/speclib_flat_quantified/mod.rs:
+// 212-333), step 1: the kept candidates' precursor rows (candidate order, not yet sorted)
+// and their fragments, flat in candidate order.
+__global__ void quant_flatten_kernel(int64_t n, int Fm, const int* nq, const int* prec_pos,
+                                     const uint64_t* frag_off, const uint64_t* pidx,
+                                     const uint64_t* rank, const uint32_t* prow, const float* rt,
+                                     const uint64_t* frow, const float* v0, const float* v1,
+                                     const float* v2, const float* v3, uint64_t* p_idx,
+                                     uint64_t* p_row, uint64_t* p_rank, float* p_rt, uint64_t* p_fs,
+                                     uint64_t* p_fe, uint32_t* p_perm, uint64_t* f_row, float* f0,
+                                     float* f1, float* f2, float* f3, uint64_t* f_pidx,
+                                     uint64_t* f_rank) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int k = nq[q];
+    if (k <= 0) continue;
+    const int j = prec_pos[q];
+    const uint64_t o = frag_off[q];
+    p_idx[j] = pidx[q];
+    p_row[j] = prow[q];
+    p_rank[j] = rank[q];
+    p_rt[j] = rt[q];
+    p_fs[j] = o;
+    p_fe[j] = o + (uint64_t)k;
+    p_perm[j] = (uint32_t)j;
+    for (int m = 0; m < k; ++m) {
+      const int64_t slot = q * Fm + m;
+      f_row[o + m] = frow[slot];
+      f0[o + m] = v0[slot];
+      f1[o + m] = v1[slot];
+      f2[o + m] = v2[slot];
+      f3[o + m] = v3[slot];
+      f_pidx[o + m] = pidx[q];
+      f_rank[o + m] = rank[q];
+    }
+  }
+}
+
+// Step 2: the precursor columns gathered in the order of the stable sort by precursor_idx.
+__global__ void quant_order_kernel(int64_t P, const uint32_t* perm, const uint64_t* row,
+                                   const uint64_t* rank, const float* rt, const uint64_t* fs,
+                                   const uint64_t* fe, uint64_t* o_row, uint64_t* o_rank,
+                                   float* o_rt, uint64_t* o_fs, uint64_t* o_fe) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < P;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = perm[j];
+    o_row[j] = row[i];
+    o_rank[j] = rank[i];
+    o_rt[j] = rt[i];
+    o_fs[j] = fs[i];
+    o_fe[j] = fe[i];
+  }
+}
+
+// Assembles the flat layout of a quantification on the device.
+int quant_assemble(AdsQuant* r, cudaStream_t st) {
+  const int64_t n = r->n, P = r->n_prec, NF = r->n_frag;
+  if (P == 0) return ADS_OK;
+  // offsets from the per-candidate counts (already on the host)
+  std::vector<int> pos((size_t)n, -1);
+  std::vector<uint64_t> off((size_t)n, 0);
+  {
+    int j = 0;
+    uint64_t o = 0;
+    for (int64_t q = 0; q < n; ++q) {
+      off[(size_t)q] = o;
+      const int k = r->nq[(size_t)q];
+      if (k > 0) {
+        pos[(size_t)q] = j++;
+        o += (uint64_t)k;
+      }
+    }
+  }
+  size_t sort_bytes = 0;
+  ADS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint64_t*)nullptr, (uint64_t*)nullptr,
+                                           (uint32_t*)nullptr, (uint32_t*)nullptr, (int)P, 0, 64, st));
+  auto rnd = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t bP8 = rnd((size_t)P * 8), bP4 = rnd((size_t)P * 4), bF8 = rnd((size_t)NF * 8),
+               bF4 = rnd((size_t)NF * 4);
+  // final columns
+  ADS_TRY(r->flat.alloc(5 * bP8 + bP4 + 3 * bF8 + 4 * bF4));
+  char* b = r->flat.p;
+  auto take = [&](size_t bytes) {
+    char* p = b;
+    b += bytes;
+    return p;
+  };
+  r->p_idx = reinterpret_cast<uint64_t*>(take(bP8));
+  r->p_row = reinterpret_cast<uint64_t*>(take(bP8));
+  r->p_rank = reinterpret_cast<uint64_t*>(take(bP8));
+  r->p_fs = reinterpret_cast<uint64_t*>(take(bP8));
+  r->p_fe = reinterpret_cast<uint64_t*>(take(bP8));
+  r->p_rt = reinterpret_cast<float*>(take(bP4));
+  r->f_row = reinterpret_cast<uint64_t*>(take(bF8));
+  r->f_pidx = reinterpret_cast<uint64_t*>(take(bF8));
+  r->f_rank = reinterpret_cast<uint64_t*>(take(bF8));
+  for (int k = 0; k < 4; ++k) r->f_val[k] = reinterpret_cast<float*>(take(bF4));
+  // temporaries: offsets, positions, unsorted precursor columns, permutation, sort space
+  const size_t bn8 = rnd((size_t)n * 8), bn4 = rnd((size_t)n * 4);
+  DevBuf<char> tmp;
+  ADS_TRY(tmp.alloc(bn8 + bn4 + 6 * bP8 + bP4 + 2 * bP4 + rnd(sort_bytes)));
+  b = tmp.p;
+  uint64_t* d_off = reinterpret_cast<uint64_t*>(take(bn8));
+  int* d_pos = reinterpret_cast<int*>(take(bn4));
+  uint64_t* u_idx = reinterpret_cast<uint64_t*>(take(bP8));
+  uint64_t* u_row = reinterpret_cast<uint64_t*>(take(bP8));
+  uint64_t* u_rank = reinterpret_cast<uint64_t*>(take(bP8));
+  uint64_t* u_fs = reinterpret_cast<uint64_t*>(take(bP8));
+  uint64_t* u_fe = reinterpret_cast<uint64_t*>(take(bP8));
+  uint64_t* u_spare = reinterpret_cast<uint64_t*>(take(bP8));
+  float* u_rt = reinterpret_cast<float*>(take(bP4));
+  uint32_t* perm_in = reinterpret_cast<uint32_t*>(take(bP4));
+  uint32_t* perm = reinterpret_cast<uint32_t*>(take(bP4));
+  void* sort_tmp = take(rnd(sort_bytes));
+  (void)u_spare;
+  ADS_CUDA(cudaMemcpyAsync(d_off, off.data(), (size_t)n * 8, cudaMemcpyHostToDevice, st));
+  ADS_CUDA(cudaMemcpyAsync(d_pos, pos.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
+  const int grid = (int)std::min<int64_t>((n + 255) / 256, 4096);
+  quant_flatten_kernel<<<grid, 256, 0, st>>>(
+      n, r->Fm, r->nq_p, d_pos, d_off, r->pidx_p, r->rank_p, r->prow_p, r->rt_p, r->frow_p,
+      r->fval_p[0], r->fval_p[1], r->fval_p[2], r->fval_p[3], u_idx, u_row, u_rank, u_rt, u_fs, u_fe,
+      perm_in, r->f_row, r->f_val[0], r->f_val[1], r->f_val[2], r->f_val[3], r->f_pidx, r->f_rank);
+  ADS_LAUNCH_CHECK();
+  // radix sort is stable: equal precursor_idx keep candidate order
+  ADS_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, u_idx, r->p_idx, perm_in, perm,
+                                           (int)P, 0, 64, st));
+  quant_order_kernel<<<(int)std::min<int64_t>((P + 255) / 256, 4096), 256, 0, st>>>(
+      P, perm, u_row, u_rank, u_rt, u_fs, u_fe, r->p_row, r->p_rank, r->p_rt, r->p_fs, r->p_fe);
+  ADS_LAUNCH_CHECK();
+  ADS_CUDA(cudaStreamSynchronize(st));
+  r->arena.release();  // the per-candidate slots are no longer needed
+  return ADS_OK;
+}
+
 // The library's IDF histogram, built once per library on the device.
 int ensure_idf(AdsLib* l, const GridView& g, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(l->mu);
@@ -1078,6 +1220,8 @@ int quant_device(const AdsQuantParams* p, const AdsDia* d, AdsLib* l, int64_t n,
       r->n_frag += v;
       r->n_prec += v > 0;
     }
+    if (r->n_prec > INT_MAX) return fail(ADS_ERR_INVALID_ARGUMENT, "too many quantified precursors");
+    ADS_TRY(quant_assemble(r.get(), st));
   }
   if (verbose) {
     // src/peak_group_quantification/mod.rs:73-78 (the kernel's device time)
@@ -1295,54 +1439,20 @@ int ads_quant_copy_out(const AdsQuant* q, uint64_t* precursor_idx, uint64_t* pre
     if (!q) return fail(ADS_ERR_INVALID_ARGUMENT, "null handle");
     if (q->n_prec == 0) return ADS_OK;
     DeviceGuard dg(q->device);
-    const size_t n = (size_t)q->n, Fm = (size_t)q->Fm;
-    std::vector<uint32_t> prow(n);
-    std::vector<float> rt(n);
-    std::vector<uint64_t> pid(n), rk(n), frow(n * Fm);
-    std::vector<float> fv[4];
-    ADS_CUDA(cudaMemcpy(prow.data(), q->prow_p, n * 4, cudaMemcpyDeviceToHost));
-    ADS_CUDA(cudaMemcpy(rt.data(), q->rt_p, n * 4, cudaMemcpyDeviceToHost));
-    ADS_CUDA(cudaMemcpy(pid.data(), q->pidx_p, n * 8, cudaMemcpyDeviceToHost));
-    ADS_CUDA(cudaMemcpy(rk.data(), q->rank_p, n * 8, cudaMemcpyDeviceToHost));
-    ADS_CUDA(cudaMemcpy(frow.data(), q->frow_p, n * Fm * 8, cudaMemcpyDeviceToHost));
-    for (int k = 0; k < 4; ++k) {
-      fv[k].resize(n * Fm);
-      ADS_CUDA(cudaMemcpy(fv[k].data(), q->fval_p[k], n * Fm * 4, cudaMemcpyDeviceToHost));
-    }
-    float* fout[4] = {intensity, mz_observed, correlation_observed, mass_error_observed};
-    // SpecLibFlatQuantified::from_precursor_quantified_vec (src/speclib_flat_quantified/
-    // mod.rs:212-333): fragments in candidate order, precursors stably sorted by idx
-    std::vector<size_t> kept;
-    std::vector<uint64_t> fs, fe;
-    uint64_t o = 0;
-    for (size_t c = 0; c < n; ++c) {
-      const int k = q->nq[c];
-      if (k <= 0) continue;
-      kept.push_back(c);
-      fs.push_back(o);
-      for (int j = 0; j < k; ++j, ++o) {
-        const size_t slot = c * Fm + (size_t)j;
-        if (fragment_row) fragment_row[o] = frow[slot];
-        for (int v = 0; v < 4; ++v)
-          if (fout[v]) fout[v][o] = fv[v][slot];
-        if (fragment_precursor_idx) fragment_precursor_idx[o] = pid[c];
-        if (fragment_rank) fragment_rank[o] = rk[c];
-      }
-      fe.push_back(o);
-    }
-    std::vector<size_t> ord(kept.size());
-    for (size_t k = 0; k < ord.size(); ++k) ord[k] = k;
-    std::stable_sort(ord.begin(), ord.end(),
-                     [&](size_t x, size_t y) { return pid[kept[x]] < pid[kept[y]]; });
-    for (size_t j = 0; j < ord.size(); ++j) {
-      const size_t k = ord[j], c = kept[k];
-      if (precursor_idx) precursor_idx[j] = pid[c];
-      if (precursor_row) precursor_row[j] = prow[c];
-      if (rank) rank[j] = rk[c];
-      if (rt_observed) rt_observed[j] = rt[c];
-      if (flat_frag_start_idx) flat_frag_start_idx[j] = fs[k];
-      if (flat_frag_stop_idx) flat_frag_stop_idx[j] = fe[k];
-    }
+    const size_t P = (size_t)q->n_prec, NF = (size_t)q->n_frag;
+    struct Col {
+      void* dst;
+      const void* src;
+      size_t bytes;
+    } cols[] = {{precursor_idx, q->p_idx, P * 8},         {precursor_row, q->p_row, P * 8},
+                {rank, q->p_rank, P * 8},                 {rt_observed, q->p_rt, P * 4},
+                {flat_frag_start_idx, q->p_fs, P * 8},    {flat_frag_stop_idx, q->p_fe, P * 8},
+                {fragment_row, q->f_row, NF * 8},         {intensity, q->f_val[0], NF * 4},
+                {mz_observed, q->f_val[1], NF * 4},       {correlation_observed, q->f_val[2], NF * 4},
+                {mass_error_observed, q->f_val[3], NF * 4}, {fragment_precursor_idx, q->f_pidx, NF * 8},
+                {fragment_rank, q->f_rank, NF * 8}};
+    for (const Col& c : cols)
+      if (c.dst) ADS_CUDA(cudaMemcpy(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost));
     return ADS_OK;
   });
 }
