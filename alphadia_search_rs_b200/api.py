@@ -821,7 +821,7 @@ class SpecLibFlatQuantified:
         return len(self._frag["mz"])
 
     def to_dict_arrays(self) -> tuple:
-        """(precursor dict, fragment dict) (src/speclib_flat_quantified/mod.rs:110-210)."""
+        """(precursor dict, fragment dict) (src/speclib_flat_quantified/mod.rs:126-210)."""
         return ({k: self._prec[k].copy() for k in _QUANT_PRECURSOR_KEYS},
                 {k: self._frag[k].copy() for k in _QUANT_FRAGMENT_KEYS})
 

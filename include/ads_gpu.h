@@ -354,7 +354,7 @@ float ads_quant_kernel_ms(const AdsQuant* quant);
  * candidate order) its row in the library's fragment arrays, observed intensity,
  * observed m/z, correlation, mass error, precursor_idx and rank.  The library's
  * pass-through columns (m/z, RT, naa, fragment annotations) are the caller's arrays at
- * those rows (src/speclib_flat_quantified/mod.rs:110-210). */
+ * those rows (src/speclib_flat_quantified/mod.rs:126-210). */
 int ads_quant_copy_out(const AdsQuant* quant, uint64_t* precursor_idx, uint64_t* precursor_row,
                        uint64_t* rank, float* rt_observed, uint64_t* flat_frag_start_idx,
                        uint64_t* flat_frag_stop_idx, uint64_t* fragment_row, float* intensity,

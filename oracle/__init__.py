@@ -501,7 +501,7 @@ QUANT_FRAGMENT_KEYS = ("mz_library", "mz", "intensity", "cardinality", "charge",
 def quantify(dia: "Dia", lb: "Lib", candidates: dict, library: dict, tolerance_ppm: float = 7.0,
              top_k_fragments: int = 10000, n_threads: int = 0):
     """PeakGroupQuantification.quantify (src/peak_group_quantification/mod.rs:49-168) as
-    SpecLibFlatQuantified.to_dict_arrays (src/speclib_flat_quantified/mod.rs:110-210):
+    SpecLibFlatQuantified.to_dict_arrays (src/speclib_flat_quantified/mod.rs:126-210):
     (precursor dict, fragment dict).  ``library`` holds the SpecLibFlat.from_arrays
     inputs, from which the pass-through columns are taken."""
     L = lib()
