@@ -246,13 +246,6 @@ __device__ void ranked_mask(const Scr& s, int64_t ev, int64_t n, int r1, int r2,
   }
 }
 
-// src/utils/mod.rs:223-237
-__device__ int64_t count_above(const Scr& s, int64_t ev, int64_t n, float thr, int64_t em) {
-  int64_t c = 0;
-  for (int64_t i = 0; i < n; ++i)
-    if ((em < 0 || s.u(em + i)) && s.f(ev + i) > thr) ++c;
-  return c;
-}
 
 // src/peak_group_scoring/utils.rs:293-312
 __device__ float gamma_ln(float x) {
@@ -521,7 +514,15 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
     const float mean_corr = F > 0 ? __fdiv_rn(rust_sum(s, CORR, F), (float)F) : 0.0f;
     const float med_corr = median_of(s, CORR, F, TMP);
     const float std_corr = std_of(s, CORR, F);
-    for (int r = 0; r < 4; ++r) ranked_mask(s, FINT, F, 6 * r, 6 * r + 6, M0 + r * Fm);
+    // create_ranked_mask(intensity, 6r, 6r + 6) for r = 0..3 from one rank per fragment:
+    // M0 holds the band rank / 6 (4: none of the four)
+    for (int64_t f = 0; f < F; ++f) {
+      const float v = s.f(FINT + f);
+      int64_t rank = 0;  // earlier not below plus later above (ties to the lower index)
+      for (int64_t j = 0; j < f; ++j) rank += !(s.f(FINT + j) < v);
+      for (int64_t j = f + 1; j < F; ++j) rank += s.f(FINT + j) > v;
+      s.su(M0 + f, (uint32_t)(rank < 24 ? rank / 6 : 4));
+    }
     for (int64_t f = 0; f < F; ++f) s.su(MATCH + f, s.f(OBS + f) > 0.0f ? 1u : 0u);
     // fragment m/z and mass errors (ppm), inverse-error weights, IDF
     for (int64_t f = 0; f < F; ++f) {
@@ -575,14 +576,36 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
     o[4 * n + q] = int_corr;
     o[5 * n + q] = (float)F;
     o[6 * n + q] = (float)(uint64_t)C;
-    o[7 * n + q] = (float)count_above(s, CORR, F, 0.95f, -1);
-    o[8 * n + q] = (float)count_above(s, CORR, F, 0.90f, -1);
-    o[9 * n + q] = (float)count_above(s, CORR, F, 0.80f, -1);
-    o[10 * n + q] = (float)count_above(s, CORR, F, 0.50f, -1);
-    o[11 * n + q] = (float)count_above(s, CORR, F, 0.0f, -1);
+    // count_values_above (src/utils/mod.rs:223-237) over the correlations, all in one
+    // pass (integer counts)
+    int c95 = 0, c90 = 0, c80 = 0, c50 = 0, c0 = 0, t0 = 0, t50 = 0;
+    int b0[4] = {0, 0, 0, 0}, b50[4] = {0, 0, 0, 0};
+    for (int64_t f = 0; f < F; ++f) {
+      const float c = s.f(CORR + f);
+      const uint32_t band = s.u(M0 + f);
+      const bool top = s.u(M6 + f) != 0u;
+      c95 += c > 0.95f;
+      c90 += c > 0.90f;
+      c80 += c > 0.80f;
+      c50 += c > 0.50f;
+      c0 += c > 0.0f;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        b0[r] += band == (uint32_t)r && c > 0.0f;
+        b50[r] += band == (uint32_t)r && c > 0.50f;
+      }
+      t0 += top && c > 0.0f;
+      t50 += top && c > 0.50f;
+    }
+    o[7 * n + q] = (float)c95;
+    o[8 * n + q] = (float)c90;
+    o[9 * n + q] = (float)c80;
+    o[10 * n + q] = (float)c50;
+    o[11 * n + q] = (float)c0;
+#pragma unroll
     for (int r = 0; r < 4; ++r) {
-      o[(12 + r) * n + q] = (float)count_above(s, CORR, F, 0.0f, M0 + r * Fm);
-      o[(16 + r) * n + q] = (float)count_above(s, CORR, F, 0.50f, M0 + r * Fm);
+      o[(12 + r) * n + q] = (float)b0[r];
+      o[(16 + r) * n + q] = (float)b50[r];
     }
     o[20 * n + q] = hyperscore(s, FTYPE, OBS, MATCH, -1, F);
     o[21 * n + q] = hyperscore(s, FTYPE, FINT, MATCH, -1, F);
@@ -603,8 +626,8 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
     o[36 * n + q] = med_sum_f;
     o[37 * n + q] = (float)F;
     o[38 * n + q] = (float)n_nz;
-    o[39 * n + q] = (float)count_above(s, CORR, F, 0.0f, M6);
-    o[40 * n + q] = (float)count_above(s, CORR, F, 0.50f, M6);
+    o[39 * n + q] = (float)t0;
+    o[40 * n + q] = (float)t50;
     a.o_pidx[q] = x;
     a.o_rank[q] = a.c_rank[q];
     a.o_found[q] = 1;
