@@ -853,7 +853,7 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
   sa.h = s->h;
   sa.k_out = k_out;
   sa.gather_mode = s->o.gather_mode;
-  sa.scan_thresh = 4 * 32 * kPrefetchChunks;
+  sa.scan_thresh = 4 * 32 * (bf16 ? kPrefetchChunks<true> : kPrefetchChunks<false>);
   sa.err = c->err_p;
   sa.cand_n = s->cand_n.p;
   sa.cand_score = s->cand_score.p;
@@ -1526,7 +1526,7 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   sa.c_max = (int)c_max;
   sa.ncell = ncell;
   sa.gather_mode = 0;
-  sa.scan_thresh = 4 * 32 * kPrefetchChunks;
+  sa.scan_thresh = 4 * 32 * kPrefetchChunks<false>;
   sa.work = work;
   sa.err = flags;
   sa.cand_n = cand_n;
