@@ -57,9 +57,11 @@ def parse():
     ap.add_argument("--cycles-per-lane", type=int, default=0)
     ap.add_argument("--gather-mode", type=int, default=0, choices=[0, 1, 2],
                     help="0 automatic, 1 scan every bin range, 2 binary-search every bin")
-    ap.add_argument("--graph", action="store_true",
-                    help="replay a captured CUDA graph per search (stage times then come "
-                         "from a second, directly enqueued pass)")
+    ap.add_argument("--graph", dest="graph", action="store_true", default=True,
+                    help="replay a captured CUDA graph per search (the default; stage times "
+                         "then come from a second, directly enqueued pass)")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="enqueue every search's kernels directly")
     ap.add_argument("--autotune", action="store_true",
                     help="pick warps per block and cycles per lane with the engine's autotuner")
     ap.add_argument("--precision", choices=["fp32", "bf16"], default=None,
