@@ -138,3 +138,54 @@ def test_edge_case_library():
     cd = candidate_dict(cand)
     assert len(cd["rank"]) > 0
     assert_quant_equal(got, oracle.quantify(od, ol, cd, la), "edge cases")
+
+
+def test_device_resident_candidate_arrays(quantified):
+    """ads_score_arrays and ads_quantify_arrays with ADS_MEM_DEVICE (candidate columns
+    already in device memory) give what the host-array calls give."""
+    import ctypes as C
+
+    import torch
+
+    from alphadia_search_rs_b200 import CandidateFeatureCollection, ScoringParameters
+    from alphadia_search_rs_b200 import _ffi as F
+
+    s = quantified
+    L = F.load()
+    c = s["cand"]
+    n = len(c["rank"])
+    dev = {k: torch.as_tensor(np.asarray(c[k]).view(np.int64) if c[k].dtype == np.uint64 else c[k],
+                              device="cuda:0") for k in COLS}
+    ptr = lambda k: dev[k].data_ptr()
+    # scoring
+    sp = ScoringParameters()._c()
+    h = C.c_void_p()
+    F.check(L.ads_score_arrays(C.byref(sp), s["dia"]._h, s["lib"]._h, n, ptr("precursor_idx"),
+                               ptr("rank"), ptr("score"), ptr("cycle_center"), ptr("cycle_start"),
+                               ptr("cycle_stop"), F.ADS_MEM_DEVICE, 0, C.byref(h)))
+    got = CandidateFeatureCollection._from_handle(h.value).to_dict_arrays()
+    from alphadia_search_rs_b200 import PeakGroupScoring
+
+    ref = PeakGroupScoring(ScoringParameters(), verbose=False).score(
+        s["dia"], s["lib"], CandidateCollection.from_arrays(*(c[k] for k in COLS))).to_dict_arrays()
+    for k in ref:
+        assert np.array_equal(np.asarray(got[k]).view(np.uint8), np.asarray(ref[k]).view(np.uint8)), k
+    # quantification
+    qp = s["qp"]._c()
+    hq = C.c_void_p()
+    F.check(L.ads_quantify_arrays(C.byref(qp), s["dia"]._h, s["lib"]._h, n, ptr("precursor_idx"),
+                                  ptr("rank"), ptr("cycle_center"), ptr("cycle_start"), ptr("cycle_stop"),
+                                  F.ADS_MEM_DEVICE, 0, C.byref(hq)))
+    try:
+        n_p, n_f = C.c_int64(), C.c_int64()
+        F.check(L.ads_quant_sizes(hq, C.byref(n_p), C.byref(n_f)))
+        rp, rf = s["got"].to_dict_arrays()
+        assert n_p.value == len(rp["precursor_idx"]) and n_f.value == len(rf["mz"])
+        out = [np.empty(max(n_p.value, 1), np.uint64) for _ in range(3)]
+        F.check(L.ads_quant_copy_out(hq, out[0].ctypes.data, None, out[1].ctypes.data, None, None,
+                                     out[2].ctypes.data, None, None, None, None, None, None, None))
+        assert np.array_equal(out[0][:n_p.value], rp["precursor_idx"])
+        assert np.array_equal(out[1][:n_p.value], rp["rank"])
+        assert np.array_equal(out[2][:n_p.value], rp["flat_frag_stop_idx"])
+    finally:
+        L.ads_quant_destroy(hq)
