@@ -476,9 +476,11 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
     }
     int64_t n_nz = 0;
     for (int64_t f = 0; f < F; ++f) n_nz += s.u(NZ + f);
-    // median profiles of all rows and of the non-zero rows (zeros when none)
+    // median profiles of all rows and of the non-zero rows (zeros when none); when every
+    // row is non-zero the two are the median of the same values
+    const bool all_nz = n_nz == F;
     for (int64_t j = 0; j < C; ++j) {
-      for (int pass = 0; pass < 2; ++pass) {
+      for (int pass = 0; pass < (all_nz ? 1 : 2); ++pass) {
         int64_t R = 0;
         for (int64_t f = 0; f < F; ++f)
           if (pass == 0 || s.u(NZ + f)) s.sf(TMP + R++, s.f(NRM + f * C + j));
@@ -489,6 +491,7 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
                            : s.f(TMP + R / 2);
         }
         s.sf((pass == 0 ? MED : MEDF) + j, med);
+        if (all_nz) s.sf(MEDF + j, med);
       }
     }
     const float med_sum = rust_sum(s, MED, C), med_sum_f = rust_sum(s, MEDF, C);
