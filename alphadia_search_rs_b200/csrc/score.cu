@@ -196,6 +196,42 @@ __device__ float correlation_safe(const Scr& s, int64_t ex, int64_t ey, int64_t 
   return fminf(fmaxf(c, -1.0f), 1.0f);
 }
 
+// correlation_safe(x, y) for many y against one x: x's sum, mean and squared deviations
+// are formed once, in the same order of operations as the one-pair form.
+struct XStats {
+  float xs, xm, xv;
+};
+
+__device__ XStats x_stats(const Scr& s, int64_t ex, int64_t n) {
+  XStats r{0.0f, 0.0f, 0.0f};
+  if (n == 0) return r;
+  r.xs = rust_sum(s, ex, n);
+  r.xm = __fdiv_rn(r.xs, (float)n);
+  for (int64_t i = 0; i < n; ++i) {
+    const float dx = __fsub_rn(s.f(ex + i), r.xm);
+    r.xv = __fadd_rn(r.xv, __fmul_rn(dx, dx));
+  }
+  return r;
+}
+
+__device__ float correlation_fixed_x(const Scr& s, const XStats& X, int64_t ex, int64_t ey,
+                                     int64_t n) {
+  if (n == 0) return 0.0f;
+  const float ys = rust_sum(s, ey, n);
+  if (X.xs == 0.0f || ys == 0.0f) return 0.0f;
+  const float ym = __fdiv_rn(ys, (float)n);
+  float yv = 0.0f, cv = 0.0f;
+  for (int64_t i = 0; i < n; ++i) {
+    const float dx = __fsub_rn(s.f(ex + i), X.xm), dy = __fsub_rn(s.f(ey + i), ym);
+    yv = __fadd_rn(yv, __fmul_rn(dy, dy));
+    cv = __fadd_rn(cv, __fmul_rn(dx, dy));
+  }
+  if (X.xv == 0.0f || yv == 0.0f) return 0.0f;
+  const float c = __fdiv_rn(cv, __fmul_rn(__fsqrt_rn(X.xv), __fsqrt_rn(yv)));
+  if (isnan(c) || isinf(c)) return 0.0f;
+  return fminf(fmaxf(c, -1.0f), 1.0f);
+}
+
 // Stable ascending insertion sort of n floats at e0 (slice::sort_by(partial_cmp)).
 __device__ void sort_floats(const Scr& s, int64_t e0, int64_t n) {
   for (int64_t i = 1; i < n; ++i) {
@@ -509,8 +545,9 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
       }
     }
     // correlations with the filtered median; observed intensities (row sums)
+    const XStats xmed = x_stats(s, MEDF, C);
     for (int64_t f = 0; f < F; ++f) {
-      s.sf(CORR + f, correlation_safe(s, MEDF, NRM + f * C, C));
+      s.sf(CORR + f, correlation_fixed_x(s, xmed, MEDF, NRM + f * C, C));
       s.sf(OBS + f, ndarray_sum(s, XIC + f * C, C));
     }
     const float int_corr = correlation_safe(s, OBS, FINT, F);
@@ -822,6 +859,7 @@ __global__ void __launch_bounds__(kScoreBlock) quant_kernel(QuantArgs qa) {
     }
     // per fragment: observed m/z and mass error, correlation, observed intensity; the
     // fragments with a positive observed intensity are kept in m/z order
+    const XStats xmed = x_stats(s, MEDF, C);
     int nq = 0;
     for (int64_t f = 0; f < F; ++f) {
       const float obs = ndarray_sum(s, XIC + f * C, C);
@@ -842,7 +880,7 @@ __global__ void __launch_bounds__(kScoreBlock) quant_kernel(QuantArgs qa) {
       qa.o_mzo[slot] = o;
       qa.o_err[slot] = o > 0.0f ? __fmul_rn(__fdiv_rn(__fsub_rn(o, lib), lib), 1e6f) : 0.0f;
       // calculate_correlation_safe(profile, median) is symmetric in its arguments
-      qa.o_corr[slot] = correlation_safe(s, MEDF, NRM + f * C, C);
+      qa.o_corr[slot] = correlation_fixed_x(s, xmed, MEDF, NRM + f * C, C);
       ++nq;
     }
     qa.o_nq[q] = nq;
