@@ -175,6 +175,9 @@ SIGNATURES = {
     "ads_quant_kernel_ms": (C.c_float, [vp]),
     "ads_quant_copy_out": (C.c_int, [vp] + [vp] * 13),
     "ads_quant_destroy": (C.c_int, [vp]),
+    "ads_idf_bins": (i64, []),
+    "ads_lib_idf_counts": (C.c_int, [vp, vp, C.c_int]),
+    "ads_lib_set_idf": (C.c_int, [vp, vp, C.c_double, C.c_int]),
 }
 
 _lib = None

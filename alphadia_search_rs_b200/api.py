@@ -305,6 +305,38 @@ class SpecLibFlat:
     def num_fragments(self) -> int:
         return self._n_frag
 
+    def idf_counts(self, out=None):
+        """Extension: the fragments of this library per m/z grid bin, the document
+        counts of scoring's IDF (src/idf/mod.rs:13-33), as a uint32 numpy array, or
+        written into ``out`` (a contiguous 32-bit CUDA tensor of ads_idf_bins()
+        elements) without leaving the device."""
+        L = _lib()
+        n = int(L.ads_idf_bins())
+        if out is not None:
+            if not _is_device_tensor(out) or out.numel() != n or out.element_size() != 4 or \
+                    not out.is_contiguous():
+                raise ValueError(f"out must be a contiguous 32-bit CUDA tensor of {n} elements")
+            F.check(L.ads_lib_idf_counts(self._h, out.data_ptr(), F.ADS_MEM_DEVICE))
+            return out
+        counts = np.empty(n, np.uint32)
+        F.check(L.ads_lib_idf_counts(self._h, counts.ctypes.data, F.ADS_MEM_HOST))
+        return counts
+
+    def set_idf(self, counts, total_fragments: int) -> None:
+        """Extension: replaces the histogram and fragment total that scoring's IDF uses
+        (the sums over the shards of a library split across ranks)."""
+        L = _lib()
+        n = int(L.ads_idf_bins())
+        if _is_device_tensor(counts):
+            if counts.numel() != n or counts.element_size() != 4 or not counts.is_contiguous():
+                raise ValueError(f"counts must be a contiguous 32-bit tensor of {n} elements")
+            F.check(L.ads_lib_set_idf(self._h, counts.data_ptr(), float(total_fragments), F.ADS_MEM_DEVICE))
+            return
+        c = np.ascontiguousarray(counts, np.uint32)
+        if c.size != n:
+            raise ValueError(f"counts must hold {n} elements")
+        F.check(L.ads_lib_set_idf(self._h, c.ctypes.data, float(total_fragments), F.ADS_MEM_HOST))
+
 
 _FLOAT_KEYS = ("fwhm_rt", "mass_tolerance", "rt_tolerance")
 _USIZE_KEYS = ("kernel_size", "peak_length", "candidate_count", "top_k_fragments")

@@ -299,6 +299,7 @@ struct AdsLib {
   // m/z grid bin, built on the first scoring call
   std::mutex mu;
   ads::DevBuf<uint32_t> idf_counts;
+  float idf_total = -1.0f;  // fragments the histogram counts (< 0: this library's own)
 };
 
 // Candidate columns on the device (CandidateCollection, src/candidate/entry.rs:41-179).

@@ -1102,7 +1102,7 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
     a.l_fnum = l->fnum_p;
     a.l_ftype = l->ftype_p;
     a.idf_counts = l->idf_counts.p;
-    a.idf_total = (float)l->n_frag;
+    a.idf_total = l->idf_total >= 0.0f ? l->idf_total : (float)l->n_frag;
     a.win = d->win_dev.p;
     a.n_obs = (int)d->n_obs;
     a.ss = d->slice_starts.p;
@@ -1526,6 +1526,43 @@ int ads_quant_destroy(AdsQuant* q) {
     if (!q) return ADS_OK;
     DeviceGuard dg(q->device);
     delete q;
+    return ADS_OK;
+  });
+}
+
+int64_t ads_idf_bins(void) {
+  return (int64_t)host_grid().size();
+}
+
+int ads_lib_idf_counts(AdsLib* lib, uint32_t* counts, int location) {
+  return guarded([&] {
+    if (!lib || !counts) return fail(ADS_ERR_INVALID_ARGUMENT, "null argument");
+    if (location != ADS_MEM_HOST && location != ADS_MEM_DEVICE)
+      return fail(ADS_ERR_INVALID_ARGUMENT, "location must be ADS_MEM_HOST or ADS_MEM_DEVICE");
+    DeviceGuard dg(lib->device);
+    GridView g;
+    ADS_TRY(device_grid(lib->device, &g));
+    ADS_TRY(ensure_idf(lib, g, cudaStreamPerThread));
+    ADS_CUDA(cudaMemcpy(counts, lib->idf_counts.p, (size_t)g.n * 4,
+                        location == ADS_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+    return ADS_OK;
+  });
+}
+
+int ads_lib_set_idf(AdsLib* lib, const uint32_t* counts, double total_fragments, int location) {
+  return guarded([&] {
+    if (!lib || !counts) return fail(ADS_ERR_INVALID_ARGUMENT, "null argument");
+    if (location != ADS_MEM_HOST && location != ADS_MEM_DEVICE)
+      return fail(ADS_ERR_INVALID_ARGUMENT, "location must be ADS_MEM_HOST or ADS_MEM_DEVICE");
+    if (!(total_fragments >= 0.0)) return fail(ADS_ERR_INVALID_ARGUMENT, "total_fragments < 0");
+    DeviceGuard dg(lib->device);
+    GridView g;
+    ADS_TRY(device_grid(lib->device, &g));
+    ADS_TRY(ensure_idf(lib, g, cudaStreamPerThread));
+    std::lock_guard<std::mutex> lk(lib->mu);
+    ADS_CUDA(cudaMemcpy(lib->idf_counts.p, counts, (size_t)g.n * 4,
+                        location == ADS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice));
+    lib->idf_total = (float)total_fragments;  // usize as f32, as the reference converts
     return ADS_OK;
   });
 }

@@ -86,3 +86,31 @@ def gather_candidates(columns: tuple, group=None, device=None) -> tuple:
         cat = np.concatenate([p[:n].cpu().numpy() for p, n in zip(parts, counts)])
         out.append(cat.view(np.uint64) if a.dtype == np.uint64 else cat)
     return tuple(out)
+
+
+def merge_idf(lib, group=None) -> None:
+    """Sharded scoring: sums the IDF histograms and fragment totals of the ranks' shards
+    of one library (the exchange step scoring needs: src/idf/mod.rs counts the fragments
+    of the whole library per m/z bin) and sets the sums on ``lib``.  ``lib`` is this
+    rank's SpecLibFlat (or anything with idf_counts / set_idf / num_fragments); the
+    counts travel as one int32 all-reduce, on the device under NCCL, on the host under
+    gloo."""
+    import torch
+    import torch.distributed as td
+
+    on_device = td.get_backend(group) == "nccl"
+    if on_device:
+        from . import _ffi
+
+        n = int(_ffi.load().ads_idf_bins())
+        counts = torch.empty(n, dtype=torch.int32, device=f"cuda:{lib.device}")
+        lib.idf_counts(out=counts)
+    else:
+        counts = torch.from_numpy(lib.idf_counts().view(np.int32).copy())
+    total = torch.tensor([lib.num_fragments], dtype=torch.int64, device=counts.device)
+    td.all_reduce(counts, op=td.ReduceOp.SUM, group=group)
+    td.all_reduce(total, op=td.ReduceOp.SUM, group=group)
+    if on_device:
+        lib.set_idf(counts, int(total.item()))
+    else:
+        lib.set_idf(counts.numpy().view(np.uint32), int(total.item()))

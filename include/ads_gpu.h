@@ -318,6 +318,17 @@ int ads_features_destroy(AdsFeatures* features);
 /* Writes up to cap feature names; returns their number (41). */
 int ads_feature_names(const char** names, int cap);
 
+/* Sharded scoring.  The IDF of scoring (src/idf/mod.rs:13-33) counts the fragments of
+ * the whole library per m/z grid bin.  A library split across ranks gives each rank's
+ * SpecLibFlat only its own counts; the ranks sum their histograms (one all-reduce of
+ * ads_idf_bins() 32-bit counts) and their fragment totals and set the sums back, after
+ * which each rank scores its candidates as the unsplit library would. */
+int64_t ads_idf_bins(void);
+/* This library's own histogram (n = ads_idf_bins()) into host or device memory. */
+int ads_lib_idf_counts(AdsLib* lib, uint32_t* counts, int location);
+/* Replaces the histogram and the fragment total scoring uses for this library. */
+int ads_lib_set_idf(AdsLib* lib, const uint32_t* counts, double total_fragments, int location);
+
 /* ---- PeakGroupQuantification (src/peak_group_quantification/mod.rs:49-168) ---- */
 
 /* QuantificationParameters (src/peak_group_quantification/parameters.rs:4-37). */

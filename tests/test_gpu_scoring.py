@@ -218,3 +218,41 @@ def test_whole_run_cycle_ranges(scored):
         s["dia"], s["lib"], CandidateCollection.from_arrays(*(c[k] for k in COLS)))
     ref = oracle.score(s["od"], s["ol"], c, log_mode=oracle.LOG_RN)
     assert_features_equal(got.to_dict_arrays(), ref, exact=True, where=s["cfg"].name + "/long")
+
+
+def test_sharded_scoring_with_merged_idf():
+    """A library split in two shards, each searched and scored on its own with the two
+    shards' IDF histograms summed (the all-reduce of a multi-GPU run, done here on one
+    GPU), gives the unsplit library's features, in the same order."""
+    import torch
+
+    from alphadia_search_rs_b200 import _ffi, sharding
+
+    cfg, lib, run = synth.make_workload("tiny_uneven", "numpy")
+    la = scoring_library(synth.library_arrays(lib), seed=8)
+    dia, whole, od, ol = build(run, la)
+    params = params_from(cfg.params_dict())
+    ref = PeakGroupScoring(ScoringParameters(), verbose=False).score(
+        dia, whole, PeakGroupSelection(params, verbose=False).search(dia, whole)).to_dict_arrays()
+    n_bins = int(_ffi.load().ads_idf_bins())
+    shards, total = [], 0
+    counts = torch.zeros(n_bins, dtype=torch.int32, device="cuda:0")
+    for r in range(2):
+        sa = sharding.shard_library(la, r, 2)
+        kw = dict(sa)
+        tol = kw.pop("precursor_rt_tolerance", None)
+        sl = SpecLibFlat.from_arrays(**kw, precursor_rt_tolerance=tol)
+        own = torch.empty(n_bins, dtype=torch.int32, device="cuda:0")
+        sl.idf_counts(out=own)
+        assert np.array_equal(own.cpu().numpy().view(np.uint32), sl.idf_counts())
+        counts += own
+        total += sl.num_fragments
+        shards.append(sl)
+    assert np.array_equal(counts.cpu().numpy().view(np.uint32), whole.idf_counts())
+    parts = []
+    for r, sl in enumerate(shards):
+        (sl.set_idf(counts, total) if r == 0 else sl.set_idf(counts.cpu().numpy().view(np.uint32), total))
+        cand = PeakGroupSelection(params, verbose=False).search(dia, sl)
+        parts.append(PeakGroupScoring(ScoringParameters(), verbose=False).score(dia, sl, cand).to_dict_arrays())
+    got = {k: np.concatenate([p[k] for p in parts]) for k in ref}
+    assert_features_equal(got, ref, exact=True, where="2 shards")

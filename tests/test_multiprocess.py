@@ -95,3 +95,62 @@ def test_shard_library_keeps_fragments():
         fs, fe = p["flat_frag_start_idx"], p["flat_frag_stop_idx"]
         assert fs[0] == 0 and fe[-1] == len(p["fragment_mz"])
         assert "precursor_rt_tolerance" in p
+
+
+class _HostIdfLib:
+    """Stands in for one rank's SpecLibFlat in the IDF merge: its own histogram of
+    fragment_mz_library over the m/z grid (find_closest_index, src/idf/mod.rs:13-33)."""
+
+    def __init__(self, fragment_mz_library):
+        import oracle
+
+        grid = oracle.ppm_index()
+        self.counts = np.zeros(len(grid), np.uint32)
+        for mz in np.asarray(fragment_mz_library, np.float32):
+            self.counts[oracle.find_closest_index(grid, float(mz))] += 1
+        self.num_fragments = len(fragment_mz_library)
+        self.set_to = None
+
+    def idf_counts(self):
+        return self.counts.copy()
+
+    def set_idf(self, counts, total):
+        self.set_to = (np.asarray(counts, np.uint32).copy(), int(total))
+
+
+def _idf_worker(rank, world, port, result_path):
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [root, os.path.join(root, "tests")]
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        cfg, lib, run = synth.make_workload("tiny", "numpy")
+        shard = sharding.shard_library(synth.library_arrays(lib), rank, world)
+        host = _HostIdfLib(shard["fragment_mz_library"])
+        sharding.merge_idf(host)
+        counts, total = host.set_to
+        np.savez(f"{result_path}.{rank}.npz", counts=counts, total=total)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_idf_merge_equals_whole_library(tmp_path):
+    """Sharded scoring's exchange step: after the all-reduce every rank holds the IDF
+    histogram and fragment total of the whole library."""
+    world, port = 2, _free_port()
+    path = str(tmp_path / "idf")
+    mp.start_processes(_idf_worker, args=(world, port, path), nprocs=world, join=True,
+                       start_method="spawn")
+    cfg, lib, run = synth.make_workload("tiny", "numpy")
+    whole = _HostIdfLib(synth.library_arrays(lib)["fragment_mz_library"])
+    for r in range(world):
+        got = np.load(f"{path}.{r}.npz")
+        assert int(got["total"]) == whole.num_fragments
+        assert np.array_equal(got["counts"], whole.counts)
