@@ -196,7 +196,7 @@ __device__ __forceinline__ uint32_t grid_find_closest(const GridView& g, float m
 
 // ln(x) of a float rounded to the nearest float: evaluated in double and rounded
 // once.  (The reference calls glibc logf, which is not correctly rounded for
-// about 1e-3 of its inputs; see the design notes.)
+// about 1e-3 of its inputs: there the two differ by one ulp.)
 __device__ __forceinline__ float ln_rn(float x) { return __double2float_rn(log((double)x)); }
 
 // The same, kept out of line for rarely taken paths (keeps hot loops small).
