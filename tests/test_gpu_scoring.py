@@ -256,3 +256,36 @@ def test_sharded_scoring_with_merged_idf():
         parts.append(PeakGroupScoring(ScoringParameters(), verbose=False).score(dia, sl, cand).to_dict_arrays())
     got = {k: np.concatenate([p[k] for p in parts]) for k in ref}
     assert_features_equal(got, ref, exact=True, where="2 shards")
+
+
+@pytest.mark.parametrize("case", ["inf_library_intensity", "huge_peaks"])
+def test_extreme_values(case):
+    """Scoring and quantification with an infinite library intensity (top-k ranks,
+    intensity correlation and hyperscore see it) or peaks near the f32 range (sums
+    overflow to inf in the XIC): device and oracle still agree bit for bit."""
+    from test_gpu_quant import assert_quant_equal, quant_library
+
+    from alphadia_search_rs_b200 import PeakGroupQuantification, QuantificationParameters
+
+    run, la = edge_case_workload()
+    la = quant_library(la, seed=11)
+    run = dict(run)
+    if case == "inf_library_intensity":
+        fi = np.array(la["fragment_intensity"], np.float32, copy=True)
+        fi[3] = np.inf
+        la["fragment_intensity"] = fi
+    else:
+        pi = np.array(run["peak_intensity"], np.float32, copy=True)
+        pi[::7] = np.float32(3e38)
+        run["peak_intensity"] = pi
+    dia, slib, od, ol = build(run, la)
+    params = dict(fwhm_rt=3.0, kernel_size=20, peak_length=5, mass_tolerance=20.0,
+                  rt_tolerance=30.0, candidate_count=3, top_k_fragments=6)
+    cand = PeakGroupSelection(params_from(params), verbose=False).search(dia, slib)
+    cd = candidate_dict(cand)
+    assert len(cd["rank"]) > 0
+    feats = PeakGroupScoring(ScoringParameters(), verbose=False).score(dia, slib, cand)
+    assert_features_equal(feats.to_dict_arrays(), oracle.score(od, ol, cd, log_mode=oracle.LOG_RN),
+                          exact=True, where=case)
+    q = PeakGroupQuantification(QuantificationParameters(), verbose=False).quantify(dia, slib, cand)
+    assert_quant_equal(q, oracle.quantify(od, ol, cd, la), case)
