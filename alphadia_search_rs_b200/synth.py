@@ -83,6 +83,11 @@ CONFIGS = {
                                (2, 4), (30.0, 160.0), 15.0, 2.0, 21, 3, 24, decoy_fraction=0.5, seed=12),
     # cfg4's search settings (kernel sigma 3 / width 31, 10 ppm, top-5, 4-24 fragments,
     # RT half-windows up to 300 cycles: several length classes, multi-pass rows)
+    # precursors with 20-60 library fragments, 40 kept: more than one warp's worth of
+    # fragments in the library preparation and the search
+    "tiny_many": SynthConfig("tiny_many", 300, 4, 25.0, 400.0, 300, 300, 20, 60, (400.0, 500.0),
+                             (2, 3), (40.0, 120.0), 15.0, 2.0, 21, 3, 40, decoy_fraction=0.3,
+                             seed=14),
     "tiny_cfg4": SynthConfig("tiny_cfg4", 700, 6, 8.0, 400.0, 400, 400, 4, 24, (400.0, 448.0),
                              (2, 4), (30.0, 300.0), 10.0, 3.0, 31, 5, 24, decoy_fraction=0.5,
                              seed=13),

@@ -18,7 +18,7 @@ from _util import (RUN_KEYS, assert_candidates_equal, edge_case_workload, oracle
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module", params=["tiny", "tiny_uneven", "tiny_cfg4", "cfg0"])
+@pytest.fixture(scope="module", params=["tiny", "tiny_uneven", "tiny_cfg4", "tiny_many", "cfg0"])
 def workload(request):
     cfg, lib, run = synth.make_workload(request.param, "numpy")
     la = synth.library_arrays(lib)

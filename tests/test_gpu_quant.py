@@ -46,7 +46,7 @@ def assert_quant_equal(got, ref, where: str):
                 raise AssertionError(f"{where}: {part} {k} differs at row {i}: {a[i]!r} vs {b[i]!r}")
 
 
-@pytest.fixture(scope="module", params=["tiny", "tiny_uneven", "tiny_cfg4", "cfg0"])
+@pytest.fixture(scope="module", params=["tiny", "tiny_uneven", "tiny_cfg4", "tiny_many", "cfg0"])
 def quantified(request):
     cfg, lib, run = synth.make_workload(request.param, "numpy")
     la = quant_library(synth.library_arrays(lib), seed=31)

@@ -82,7 +82,7 @@ def assert_features_equal(got: dict, ref: dict, exact: bool, where: str):
     assert not report, f"{where}:\n  " + "\n  ".join(report)
 
 
-@pytest.fixture(scope="module", params=["tiny", "tiny_uneven", "tiny_cfg4", "cfg0"])
+@pytest.fixture(scope="module", params=["tiny", "tiny_uneven", "tiny_cfg4", "tiny_many", "cfg0"])
 def scored(request):
     """Search on the device, score the collection still on the device, and the
     oracle's features of the same candidates."""
