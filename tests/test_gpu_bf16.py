@@ -47,6 +47,7 @@ def compare_to_fp64(got: dict, ref: dict):
 
 
 @pytest.mark.parametrize("name,min_agree", [("tiny", 0.99), ("tiny_uneven", 0.99), ("tiny_cfg4", 0.99),
+                                            ("tiny_many", 0.99),
                                             ("cfg0", 0.995)])
 def test_bf16_against_fp64_oracle(name, min_agree):
     cfg, lib, run = synth.make_workload(name, "numpy")

@@ -289,3 +289,46 @@ def test_extreme_values(case):
                           exact=True, where=case)
     q = PeakGroupQuantification(QuantificationParameters(), verbose=False).quantify(dia, slib, cand)
     assert_quant_equal(q, oracle.quantify(od, ol, cd, la), case)
+
+
+def test_concurrent_threads_share_run_and_library():
+    """Four host threads search, score and quantify against the same DIAData and
+    SpecLibFlat at once (each call on its thread's stream; the library's IDF histogram
+    is built once under a lock); every thread gets the serial result."""
+    import threading
+
+    from test_gpu_quant import quant_library
+
+    from alphadia_search_rs_b200 import PeakGroupQuantification, QuantificationParameters
+
+    cfg, lib, run = synth.make_workload("tiny_uneven", "numpy")
+    la = quant_library(synth.library_arrays(lib), seed=2)
+    dia, slib, od, ol = build(run, la)
+    params = params_from(cfg.params_dict())
+
+    def job():
+        cand = PeakGroupSelection(params, verbose=False).search(dia, slib)
+        f = PeakGroupScoring(ScoringParameters(), verbose=False).score(dia, slib, cand).to_dict_arrays()
+        q = PeakGroupQuantification(QuantificationParameters(), verbose=False).quantify(dia, slib, cand)
+        return f, q.to_dict_arrays()
+
+    results, errors = [None] * 4, []
+
+    def run_one(i):
+        try:
+            results[i] = job()
+        except Exception as e:  # reported below
+            errors.append(repr(e))
+
+    threads = [threading.Thread(target=run_one, args=(i,)) for i in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    ref_f, ref_q = job()
+    for f, q in results:
+        assert_features_equal(f, ref_f, exact=True, where="thread")
+        for part, g, r in ((0, q[0], ref_q[0]), (1, q[1], ref_q[1])):
+            for k in r:
+                assert np.array_equal(np.asarray(g[k]).view(np.uint8), np.asarray(r[k]).view(np.uint8)), (part, k)
