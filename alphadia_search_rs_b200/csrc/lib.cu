@@ -86,7 +86,7 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
   DeviceGuard dg(device);
   const int L = a->location;
 
-  // validation of the per-precursor arrays (the reference panics on these)
+  // host views of the per-precursor arrays the host validates below
   std::vector<uint64_t> fs_store, fe_store;
   std::vector<float> rt_store, tol_store;
   const uint64_t *fs = nullptr, *fe = nullptr;
@@ -98,25 +98,7 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
   lib->device = device;
   lib->n_prec = P;
   lib->n_frag = NF;
-  for (int64_t i = 0; i < P; ++i) {
-    if (fs[i] > fe[i] || fe[i] > (uint64_t)NF)
-      return fail(ADS_ERR_INVALID_ARGUMENT,
-                  "precursor " + std::to_string(i) + ": fragment range outside [0, n_fragments]");
-    if (!std::isfinite(prt[i]))
-      return fail(ADS_ERR_INVALID_ARGUMENT, "precursor " + std::to_string(i) + ": RT is not finite");
-    lib->max_frag = std::max<int64_t>(lib->max_frag, (int64_t)(fe[i] - fs[i]));
-  }
-  if (a->precursor_rt_tolerance) {
-    ADS_TRY(host_view(a->precursor_rt_tolerance, P, L, tol_store, &tol));
-    lib->has_tol = true;
-    for (int64_t i = 0; i < P; ++i) {
-      const float v = tol[i];
-      if (std::isfinite(v))
-        lib->max_tol = std::max(lib->max_tol, v);
-      else if (!std::isnan(v))
-        lib->max_tol = INFINITY;
-    }
-  }
+  lib->has_tol = a->precursor_rt_tolerance != nullptr;
 
   cudaStream_t st;
   ADS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -196,6 +178,28 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
   ADS_TRY(copy_in(lib->fint_p, a->fragment_intensity, NF, L, st));
   ADS_TRY(copy_in(lib->fnum_p, a->fragment_number, NF, L, st));
   ADS_TRY(copy_in(lib->ftype_p, a->fragment_type, NF, L, st));
+
+  // validation of the per-precursor arrays (the reference panics on these), on the
+  // host while the copies above are in flight; on failure the buffers are released
+  // only after the device is idle
+  for (int64_t i = 0; i < P; ++i) {
+    if (fs[i] > fe[i] || fe[i] > (uint64_t)NF)
+      return fail(ADS_ERR_INVALID_ARGUMENT,
+                  "precursor " + std::to_string(i) + ": fragment range outside [0, n_fragments]");
+    if (!std::isfinite(prt[i]))
+      return fail(ADS_ERR_INVALID_ARGUMENT, "precursor " + std::to_string(i) + ": RT is not finite");
+    lib->max_frag = std::max<int64_t>(lib->max_frag, (int64_t)(fe[i] - fs[i]));
+  }
+  if (a->precursor_rt_tolerance) {
+    ADS_TRY(host_view(a->precursor_rt_tolerance, P, L, tol_store, &tol));
+    for (int64_t i = 0; i < P; ++i) {
+      const float v = tol[i];
+      if (std::isfinite(v))
+        lib->max_tol = std::max(lib->max_tol, v);
+      else if (!std::isnan(v))
+        lib->max_tol = INFINITY;
+    }
+  }
 
   if (sort) {
     // stable radix sort of (precursor_idx, position): equal keys keep input order

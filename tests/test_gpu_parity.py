@@ -232,3 +232,30 @@ def test_statistics_pass_counts(workload):
     assert st["fragments"] > 0
     assert st["fragments"] <= st["xic_cells"] <= st["fragments"] * n_cycles
     assert st["entries_accumulated"] <= st["entries_read"]
+
+
+@pytest.mark.parametrize("where", ["host", "device"])
+@pytest.mark.parametrize("fault", ["range", "rt_nan", "rt_inf"])
+def test_library_validation(where, fault):
+    """SpecLibFlat.from_arrays rejects what the reference would panic on (a fragment
+    range outside the fragment arrays, a non-finite precursor RT) with ValueError,
+    for host arrays and for CUDA tensors, and the library built afterwards works."""
+    import torch
+
+    from alphadia_search_rs_b200 import SpecLibFlat
+
+    cfg, lib, run = synth.make_workload("tiny", "numpy")
+    la = {k: np.array(v, copy=True) for k, v in synth.library_arrays(lib).items()}
+    if fault == "range":
+        la["flat_frag_stop_idx"][5] = np.uint64(len(la["fragment_mz"]) + 3)
+    else:
+        la["precursor_rt"][7] = np.float32(np.nan if fault == "rt_nan" else np.inf)
+    if where == "device":
+        la = {k: torch.as_tensor(v.view(np.int64) if v.dtype == np.uint64 else v, device="cuda:0")
+              for k, v in la.items()}
+        for k in ("precursor_idx", "flat_frag_start_idx", "flat_frag_stop_idx"):
+            la[k] = la[k].view(torch.uint64)
+    with pytest.raises(ValueError, match="fragment range|RT is not finite"):
+        SpecLibFlat.from_arrays(**la)
+    ok = SpecLibFlat.from_arrays(**synth.library_arrays(lib))
+    assert ok.num_precursors == len(synth.library_arrays(lib)["precursor_idx"])
