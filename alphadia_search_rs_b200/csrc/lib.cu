@@ -138,7 +138,15 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
   uint8_t* naa_in = nullptr;
   void* sort_tmp = nullptr;
   size_t sort_bytes = 0;
-  const bool sort = P > 1;
+  // host arrays already in precursor_idx order (non-decreasing) need no sort: the
+  // stable sort would keep them as they are
+  bool in_order = false;
+  if (L == ADS_MEM_HOST && P > 1 && a->precursor_idx) {
+    const uint64_t* pi = a->precursor_idx;
+    in_order = true;
+    for (int64_t i = 1; i < P && in_order; ++i) in_order = pi[i - 1] <= pi[i];
+  }
+  const bool sort = P > 1 && !in_order;
   if (sort) {
     ADS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint64_t*)nullptr,
                                              (uint64_t*)nullptr, (uint32_t*)nullptr,
@@ -215,8 +223,9 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     launch_gather(P, pos_out, naa_in, lib->naa_p, st);
     if (lib->has_tol) launch_gather(P, pos_out, ptol_in, lib->ptol_p, st);
     ADS_LAUNCH_CHECK();
-  } else if (P == 1) {
-    ADS_CUDA(cudaMemsetAsync(lib->prow_p, 0, sizeof(uint32_t), st));
+  } else if (P > 0) {
+    iota_kernel<<<(int)std::min<int64_t>((P + 255) / 256, 4096), 256, 0, st>>>(P, lib->prow_p);
+    ADS_LAUNCH_CHECK();
   }
   ADS_CUDA(cudaStreamSynchronize(st));
   *out = lib.release();
