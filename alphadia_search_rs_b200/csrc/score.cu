@@ -368,6 +368,124 @@ __global__ void cycle_span_kernel(int64_t n, const uint64_t* center, const uint6
   }
 }
 
+// ---- per-candidate steps shared by the scoring and quantification kernels
+
+// filter_sort_fragments (src/speclib_flat/mod.rs:240-345) of the precursor's nraw
+// library fragments from fs: kept when non-zero and not y1; the top_k by intensity
+// (ties to the lower position); in m/z order (ties keep library order).  Writes the
+// kept fragments' m/z to FMZ and their library offsets (from fs) to FRAW; returns F.
+__device__ __forceinline__ int64_t select_fragments(const ScoreArgs& a, const Scr& s, int64_t KEEP,
+                                                    int64_t FMZ, int64_t FRAW, int64_t fs,
+                                                    int64_t nraw) {
+  int64_t nk = 0;
+  for (int64_t r = 0; r < nraw; ++r) {
+    const float I = a.l_fint[fs + r];
+    const bool k = I > 0.0f && !(a.l_ftype[fs + r] == 121 && a.l_fnum[fs + r] == 1);
+    s.su(KEEP + r, k ? 1u : 0u);
+    nk += k;
+  }
+  const bool topk = nk > a.top_k;
+  if (topk) {
+    for (int64_t r = 0; r < nraw; ++r) {
+      if (!s.u(KEEP + r)) continue;
+      const float I = a.l_fint[fs + r];
+      int64_t rank = 0;  // earlier not below plus later above
+      for (int64_t j = 0; j < r; ++j)
+        if (s.u(KEEP + j)) rank += !(a.l_fint[fs + j] < I);
+      for (int64_t j = r + 1; j < nraw; ++j)
+        if (s.u(KEEP + j)) rank += a.l_fint[fs + j] > I;
+      if (rank < a.top_k) s.su(KEEP + r, 2u);
+    }
+  }
+  const uint32_t need = topk ? 2u : 1u;
+  for (int64_t r = 0; r < nraw; ++r) {
+    if (s.u(KEEP + r) < need) continue;
+    const float m = a.l_fmz[fs + r];
+    int64_t pos = 0;  // stable: ties keep their library order
+    for (int64_t j = 0; j < r; ++j)
+      if (s.u(KEEP + j) >= need) pos += !(a.l_fmz[fs + j] > m);
+    for (int64_t j = r + 1; j < nraw; ++j)
+      if (s.u(KEEP + j) >= need) pos += a.l_fmz[fs + j] < m;
+    s.sf(FMZ + pos, m);
+    s.su(FRAW + pos, (uint32_t)r);
+  }
+  return topk ? a.top_k : nk;
+}
+
+// DenseXICMZObservation::new (src/dense_xic_observation/mod.rs:97-137) over cycles
+// [cs, ce): the F x C dense XIC and intensity-weighted m/z matrices, every window that
+// holds the precursor m/z in order, bins in order, entries in cycle order, with Rust's
+// binary_search landing on the last entry at the first cycle
+// (src/quadrupole_observation/mod.rs:152-211).
+__device__ __forceinline__ void gather_xic_mz(const ScoreArgs& a, const Scr& s, int64_t XIC,
+                                              int64_t MZO, int64_t FMZ, int64_t F, int cs, int ce,
+                                              float pmz) {
+  const int64_t C = ce - cs;
+  for (int64_t e = 0; e < F * C; ++e) {
+    s.sf(XIC + e, 0.0f);
+    s.sf(MZO + e, 0.0f);
+  }
+  for (int w = 0; w < a.n_obs; ++w) {
+    const WinInfo wi = a.win[w];
+    if (!(wi.lo <= pmz && wi.hi >= pmz) || wi.ss_off < 0) continue;  // empty: no peaks
+    const uint32_t* ssw = a.ss + wi.ss_off;
+    const uint16_t* cyw = a.cyc + wi.base;
+    const float* inw = a.inten + wi.base;
+    for (int64_t f = 0; f < F; ++f) {
+      const float mz = s.f(FMZ + f);
+      const float delta = __fmul_rn(__fmul_rn(mz, a.tol), 1e-6f);
+      const uint32_t b0 = grid_lower_bound(a.g, __fsub_rn(mz, delta));
+      const uint32_t b1 = max(b0, grid_upper_bound(a.g, __fadd_rn(mz, delta)));
+      for (uint32_t b = b0; b < b1; ++b) {
+        const float actual = __ldg(a.g.grid + b);
+        const int64_t e0 = ssw[b], e1 = ssw[b + 1];
+        for (int64_t k = e0 + bsearch_u16_rust(cyw + e0, e1 - e0, cs); k < e1; ++k) {
+          const int c = cyw[k];
+          if (c >= ce) break;
+          const int64_t at = f * C + (c - cs);
+          const float v = inw[k];
+          const float xs = __fadd_rn(s.f(XIC + at), v);
+          s.sf(XIC + at, xs);
+          if (v > 0.0f) {
+            const float prev = __fsub_rn(xs, v);
+            if (prev == 0.0f)
+              s.sf(MZO + at, actual);
+            else
+              s.sf(MZO + at, __fdiv_rn(__fadd_rn(__fmul_rn(s.f(MZO + at), prev),
+                                                 __fmul_rn(actual, v)),
+                                       xs));
+          }
+        }
+      }
+    }
+  }
+}
+
+// normalize_profiles(xic, 1) (src/peak_group_scoring/utils.rs:71-109) into NRM, and per
+// row whether it stays non-zero (NZ).
+__device__ __forceinline__ void normalize_rows(const Scr& s, int64_t XIC, int64_t NRM, int64_t NZ,
+                                               int64_t F, int64_t C) {
+  const int64_t center_c = C / 2;
+  const int64_t c0 = center_c > 1 ? center_c - 1 : 0;
+  const int64_t c1 = center_c + 2 < C ? center_c + 2 : C;
+  for (int64_t f = 0; f < F; ++f) {
+    float sum = 0.0f;
+    int64_t count = 0;
+    for (int64_t j = c0; j < c1; ++j) {
+      sum = __fadd_rn(sum, s.f(XIC + f * C + j));
+      ++count;
+    }
+    const float mean = count > 0 ? __fdiv_rn(sum, (float)count) : 0.0f;
+    uint32_t nz = 0;
+    for (int64_t j = 0; j < C; ++j) {
+      const float v = mean > 0.0f ? __fdiv_rn(s.f(XIC + f * C + j), mean) : 0.0f;
+      s.sf(NRM + f * C + j, v);
+      nz |= v != 0.0f;
+    }
+    s.su(NZ + f, nz);
+  }
+}
+
 __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= a.T) return;
@@ -377,9 +495,9 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
   const int64_t XIC = 0, MZO = Fm * Cm, NRM = 2 * Fm * Cm, V = 3 * Fm * Cm;
   const int64_t FMZ = V, FMZL = V + Fm, FINT = V + 2 * Fm, FTYPE = V + 3 * Fm, FNUM = V + 4 * Fm,
                 OBS = V + 5 * Fm, CORR = V + 6 * Fm, ERR = V + 7 * Fm, IDF = V + 8 * Fm,
-                INVW = V + 9 * Fm, M0 = V + 10 * Fm, MATCH = V + 14 * Fm, M6 = V + 15 * Fm,
-                TMP = V + 16 * Fm, NZ = V + 17 * Fm, MED = V + 18 * Fm, MEDF = MED + Cm,
-                KEEP = MEDF + Cm;
+                INVW = V + 9 * Fm, M0 = V + 10 * Fm, FRAW = V + 11 * Fm, MATCH = V + 14 * Fm,
+                M6 = V + 15 * Fm, TMP = V + 16 * Fm, NZ = V + 17 * Fm, MED = V + 18 * Fm,
+                MEDF = MED + Cm, KEEP = MEDF + Cm;
 
   for (int64_t q = t; q < a.n; q += a.T) {
     a.o_found[q] = 0;
@@ -403,113 +521,24 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
       if (a.l_pidx[base] != x) continue;  // skipped, as in the reference
       i = base;
     }
-    // filter_sort_fragments: non-zero, no y1, top-k by intensity (ties to the lower
-    // position), sorted by m/z (ties by position)
+    // filter_sort_fragments, then the kept fragments' library columns
     const int64_t fs = (int64_t)a.l_fs[i], nraw = (int64_t)a.l_fe[i] - fs;
     if (nraw > a.Fraw) {
       atomicOr(a.err, 2);
       continue;
     }
-    int64_t nk = 0;
-    for (int64_t r = 0; r < nraw; ++r) {
-      const float I = a.l_fint[fs + r];
-      const bool k = I > 0.0f && !(a.l_ftype[fs + r] == 121 && a.l_fnum[fs + r] == 1);
-      s.su(KEEP + r, k ? 1u : 0u);
-      nk += k;
+    const int64_t F = select_fragments(a, s, KEEP, FMZ, FRAW, fs, nraw);
+    for (int64_t f = 0; f < F; ++f) {
+      const int64_t r = fs + (int64_t)s.u(FRAW + f);
+      s.sf(FMZL + f, a.l_fmzl[r]);
+      s.sf(FINT + f, a.l_fint[r]);
+      s.su(FTYPE + f, a.l_ftype[r]);
+      s.su(FNUM + f, a.l_fnum[r]);
     }
-    const bool topk = nk > a.top_k;
-    if (topk) {
-      for (int64_t r = 0; r < nraw; ++r) {
-        if (!s.u(KEEP + r)) continue;
-        const float I = a.l_fint[fs + r];
-        int64_t rank = 0;  // ties to the lower position, as ranked_mask
-        for (int64_t j = 0; j < r; ++j)
-          if (s.u(KEEP + j)) rank += !(a.l_fint[fs + j] < I);
-        for (int64_t j = r + 1; j < nraw; ++j)
-          if (s.u(KEEP + j)) rank += a.l_fint[fs + j] > I;
-        if (rank < a.top_k) s.su(KEEP + r, 2u);
-      }
-    }
-    const uint32_t need = topk ? 2u : 1u;
-    const int64_t F = topk ? a.top_k : nk;
-    for (int64_t r = 0; r < nraw; ++r) {
-      if (s.u(KEEP + r) < need) continue;
-      const float m = a.l_fmz[fs + r];
-      int64_t pos = 0;  // stable: ties keep their library order
-      for (int64_t j = 0; j < r; ++j)
-        if (s.u(KEEP + j) >= need) pos += !(a.l_fmz[fs + j] > m);
-      for (int64_t j = r + 1; j < nraw; ++j)
-        if (s.u(KEEP + j) >= need) pos += a.l_fmz[fs + j] < m;
-      s.sf(FMZ + pos, m);
-      s.sf(FMZL + pos, a.l_fmzl[fs + r]);
-      s.sf(FINT + pos, a.l_fint[fs + r]);
-      s.su(FTYPE + pos, a.l_ftype[fs + r]);
-      s.su(FNUM + pos, a.l_fnum[fs + r]);
-    }
-    // DenseXICMZObservation::new over the candidate's cycles
     const int cs = (int)cs64, ce = (int)ce64;
     const int64_t C = ce - cs;
-    for (int64_t e = 0; e < F * C; ++e) {
-      s.sf(XIC + e, 0.0f);
-      s.sf(MZO + e, 0.0f);
-    }
-    const float pmz = a.l_pmz[i];
-    for (int w = 0; w < a.n_obs; ++w) {
-      const WinInfo wi = a.win[w];
-      if (!(wi.lo <= pmz && wi.hi >= pmz) || wi.ss_off < 0) continue;  // empty: no peaks
-      const uint32_t* ssw = a.ss + wi.ss_off;
-      const uint16_t* cyw = a.cyc + wi.base;
-      const float* inw = a.inten + wi.base;
-      for (int64_t f = 0; f < F; ++f) {
-        const float mz = s.f(FMZ + f);
-        const float delta = __fmul_rn(__fmul_rn(mz, a.tol), 1e-6f);
-        const uint32_t b0 = grid_lower_bound(a.g, __fsub_rn(mz, delta));
-        const uint32_t b1 = max(b0, grid_upper_bound(a.g, __fadd_rn(mz, delta)));
-        for (uint32_t b = b0; b < b1; ++b) {
-          const float actual = __ldg(a.g.grid + b);
-          const int64_t e0 = ssw[b], e1 = ssw[b + 1];
-          for (int64_t k = e0 + bsearch_u16_rust(cyw + e0, e1 - e0, cs); k < e1; ++k) {
-            const int c = cyw[k];
-            if (c >= ce) break;
-            const int64_t at = f * C + (c - cs);
-            const float v = inw[k];
-            const float xs = __fadd_rn(s.f(XIC + at), v);
-            s.sf(XIC + at, xs);
-            if (v > 0.0f) {
-              const float prev = __fsub_rn(xs, v);
-              if (prev == 0.0f)
-                s.sf(MZO + at, actual);
-              else
-                s.sf(MZO + at, __fdiv_rn(__fadd_rn(__fmul_rn(s.f(MZO + at), prev),
-                                                   __fmul_rn(actual, v)),
-                                         xs));
-            }
-          }
-        }
-      }
-    }
-    // normalize_profiles(xic, 1) and the rows that stay non-zero
-    {
-      const int64_t center_c = C / 2;
-      const int64_t c0 = center_c > 1 ? center_c - 1 : 0;
-      const int64_t c1 = center_c + 2 < C ? center_c + 2 : C;
-      for (int64_t f = 0; f < F; ++f) {
-        float sum = 0.0f;
-        int64_t count = 0;
-        for (int64_t j = c0; j < c1; ++j) {
-          sum = __fadd_rn(sum, s.f(XIC + f * C + j));
-          ++count;
-        }
-        const float mean = count > 0 ? __fdiv_rn(sum, (float)count) : 0.0f;
-        uint32_t nz = 0;
-        for (int64_t j = 0; j < C; ++j) {
-          const float v = mean > 0.0f ? __fdiv_rn(s.f(XIC + f * C + j), mean) : 0.0f;
-          s.sf(NRM + f * C + j, v);
-          nz |= v != 0.0f;
-        }
-        s.su(NZ + f, nz);
-      }
-    }
+    gather_xic_mz(a, s, XIC, MZO, FMZ, F, cs, ce, a.l_pmz[i]);
+    normalize_rows(s, XIC, NRM, NZ, F, C);
     int64_t n_nz = 0;
     for (int64_t f = 0; f < F; ++f) n_nz += s.u(NZ + f);
     // median profiles of all rows and of the non-zero rows (zeros when none); when every
@@ -747,103 +776,11 @@ __global__ void __launch_bounds__(kScoreBlock) quant_kernel(QuantArgs qa) {
       atomicOr(a.err, 2);
       continue;
     }
-    int64_t nk = 0;
-    for (int64_t r = 0; r < nraw; ++r) {
-      const float I = a.l_fint[fs + r];
-      const bool k = I > 0.0f && !(a.l_ftype[fs + r] == 121 && a.l_fnum[fs + r] == 1);
-      s.su(KEEP + r, k ? 1u : 0u);
-      nk += k;
-    }
-    const bool topk = nk > a.top_k;
-    if (topk) {
-      for (int64_t r = 0; r < nraw; ++r) {
-        if (!s.u(KEEP + r)) continue;
-        const float I = a.l_fint[fs + r];
-        int64_t rank = 0;  // ties to the lower position
-        for (int64_t j = 0; j < r; ++j)
-          if (s.u(KEEP + j)) rank += !(a.l_fint[fs + j] < I);
-        for (int64_t j = r + 1; j < nraw; ++j)
-          if (s.u(KEEP + j)) rank += a.l_fint[fs + j] > I;
-        if (rank < a.top_k) s.su(KEEP + r, 2u);
-      }
-    }
-    const uint32_t need = topk ? 2u : 1u;
-    const int64_t F = topk ? a.top_k : nk;
-    for (int64_t r = 0; r < nraw; ++r) {
-      if (s.u(KEEP + r) < need) continue;
-      const float m = a.l_fmz[fs + r];
-      int64_t pos = 0;  // stable: ties keep their library order
-      for (int64_t j = 0; j < r; ++j)
-        if (s.u(KEEP + j) >= need) pos += !(a.l_fmz[fs + j] > m);
-      for (int64_t j = r + 1; j < nraw; ++j)
-        if (s.u(KEEP + j) >= need) pos += a.l_fmz[fs + j] < m;
-      s.sf(FMZ + pos, m);
-      s.su(FRAW + pos, (uint32_t)r);
-    }
-    // DenseXICMZObservation::new over the candidate's cycles
+    const int64_t F = select_fragments(a, s, KEEP, FMZ, FRAW, fs, nraw);
     const int cs = (int)cs64, ce = (int)ce64;
     const int64_t C = ce - cs;
-    for (int64_t e = 0; e < F * C; ++e) {
-      s.sf(XIC + e, 0.0f);
-      s.sf(MZO + e, 0.0f);
-    }
-    const float pmz = a.l_pmz[i];
-    for (int w = 0; w < a.n_obs; ++w) {
-      const WinInfo wi = a.win[w];
-      if (!(wi.lo <= pmz && wi.hi >= pmz) || wi.ss_off < 0) continue;  // empty: no peaks
-      const uint32_t* ssw = a.ss + wi.ss_off;
-      const uint16_t* cyw = a.cyc + wi.base;
-      const float* inw = a.inten + wi.base;
-      for (int64_t f = 0; f < F; ++f) {
-        const float mz = s.f(FMZ + f);
-        const float delta = __fmul_rn(__fmul_rn(mz, a.tol), 1e-6f);
-        const uint32_t b0 = grid_lower_bound(a.g, __fsub_rn(mz, delta));
-        const uint32_t b1 = max(b0, grid_upper_bound(a.g, __fadd_rn(mz, delta)));
-        for (uint32_t b = b0; b < b1; ++b) {
-          const float actual = __ldg(a.g.grid + b);
-          const int64_t e0 = ssw[b], e1 = ssw[b + 1];
-          for (int64_t k = e0 + bsearch_u16_rust(cyw + e0, e1 - e0, cs); k < e1; ++k) {
-            const int c = cyw[k];
-            if (c >= ce) break;
-            const int64_t at = f * C + (c - cs);
-            const float v = inw[k];
-            const float xs = __fadd_rn(s.f(XIC + at), v);
-            s.sf(XIC + at, xs);
-            if (v > 0.0f) {
-              const float prev = __fsub_rn(xs, v);
-              if (prev == 0.0f)
-                s.sf(MZO + at, actual);
-              else
-                s.sf(MZO + at, __fdiv_rn(__fadd_rn(__fmul_rn(s.f(MZO + at), prev),
-                                                   __fmul_rn(actual, v)),
-                                         xs));
-            }
-          }
-        }
-      }
-    }
-    // normalize_profiles(xic, 1) and the rows that stay non-zero
-    {
-      const int64_t center_c = C / 2;
-      const int64_t c0 = center_c > 1 ? center_c - 1 : 0;
-      const int64_t c1 = center_c + 2 < C ? center_c + 2 : C;
-      for (int64_t f = 0; f < F; ++f) {
-        float sum = 0.0f;
-        int64_t count = 0;
-        for (int64_t j = c0; j < c1; ++j) {
-          sum = __fadd_rn(sum, s.f(XIC + f * C + j));
-          ++count;
-        }
-        const float mean = count > 0 ? __fdiv_rn(sum, (float)count) : 0.0f;
-        uint32_t nz = 0;
-        for (int64_t j = 0; j < C; ++j) {
-          const float v = mean > 0.0f ? __fdiv_rn(s.f(XIC + f * C + j), mean) : 0.0f;
-          s.sf(NRM + f * C + j, v);
-          nz |= v != 0.0f;
-        }
-        s.su(NZ + f, nz);
-      }
-    }
+    gather_xic_mz(a, s, XIC, MZO, FMZ, F, cs, ce, a.l_pmz[i]);
+    normalize_rows(s, XIC, NRM, NZ, F, C);
     // filter_non_zero + median_axis_0 (zeros when no row is non-zero)
     for (int64_t j = 0; j < C; ++j) {
       int64_t R = 0;
