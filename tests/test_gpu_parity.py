@@ -259,3 +259,17 @@ def test_library_validation(where, fault):
         SpecLibFlat.from_arrays(**la)
     ok = SpecLibFlat.from_arrays(**synth.library_arrays(lib))
     assert ok.num_precursors == len(synth.library_arrays(lib)["precursor_idx"])
+
+
+@pytest.mark.parametrize("top_k", [6, 12, 32, 33, 60])
+def test_many_fragments_top_k(top_k):
+    """Precursors with 20-60 library fragments searched with top-k below, at and above
+    one warp's worth of fragments: the library preparation's multi-pass selection and
+    the search kernel's fragments past the first 32 stay bit-exact."""
+    cfg, lib, run = synth.make_workload("tiny_many", "numpy")
+    la = synth.library_arrays(lib)
+    params = dict(cfg.params_dict(), top_k_fragments=top_k)
+    got, *_ = product_search(run, la, params)
+    ref = oracle_search(run, la, params, oracle.LOG_RN)
+    assert len(ref["rank"]) > 0
+    assert_candidates_equal(got, ref, exact_scores=True, where=f"top-{top_k}")
