@@ -57,10 +57,11 @@ struct SearchArgs {
 };
 
 // CSR entries read per round trip of the scanning gather: 2 x 32 for f32 intensities,
-// 4 x 32 for bfloat16 ones (measured: 64-entry batches are 3.7 % faster on 3000 x 300
-// FP32 data with 301-cycle windows, 128-entry batches 3 % faster for BF16 storage).
+// 3 x 32 for bfloat16 ones (measured: 64-entry batches are 3.7 % faster than 128 on
+// 3000 x 300 FP32 data with 301-cycle windows; for BF16 storage 96-entry batches are
+// 0.5-1 % faster than 128, 64 and 192 slower).
 template <bool FAST>
-constexpr int kPrefetchChunks = FAST ? 4 : 2;
+constexpr int kPrefetchChunks = FAST ? 3 : 2;
 constexpr int kBitOff = 32;         // bitmap bit of cycle c is c + kBitOff (room for -h)
 constexpr int kMaxCycles = 2048;    // longest RT window (cycles) a precursor may span
 constexpr int kTouchCap = 256;      // cells a row records for clearing; beyond it the row is
