@@ -167,6 +167,9 @@ int device_grid(int device, GridView* out) {
   ADS_CUDA(cudaMalloc(&st.lut, n_lut * sizeof(uint32_t)));
   ADS_CUDA(cudaMemcpy(st.grid, g.data(), n * sizeof(float), cudaMemcpyHostToDevice));
   ADS_CUDA(cudaMemcpy(st.lut, lut.data(), n_lut * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  // copies from pageable memory may return before their DMA ends, and the kernels
+  // that read the grid run on non-blocking streams
+  ADS_CUDA(cudaDeviceSynchronize());
   st.view.grid = st.grid;
   st.view.lut = st.lut;
   st.view.n = n;
@@ -206,6 +209,7 @@ int device_ln_table(int device, const double2** out) {
   double2* d = nullptr;
   ADS_CUDA(cudaMalloc(&d, kLnTableSize * sizeof(double2)));
   ADS_CUDA(cudaMemcpy(d, tab.data(), kLnTableSize * sizeof(double2), cudaMemcpyHostToDevice));
+  ADS_CUDA(cudaDeviceSynchronize());  // as for the grid: the DMA has landed before any use
   g_ln_tables[device] = d;
   *out = d;
   return ADS_OK;

@@ -348,6 +348,9 @@ int dia_create(const AdsRawArrays* raw, int device, AdsDia** out) {
     ADS_CUDA(cudaMemcpy(d->win_dev.p, d->win.data(), n_obs * sizeof(WinInfo), cudaMemcpyHostToDevice));
   ADS_TRY(d->rt_dev.alloc(std::max<int64_t>(n_rt, 1)));
   if (n_rt) ADS_CUDA(cudaMemcpy(d->rt_dev.p, d->rt.data(), n_rt * 4, cudaMemcpyHostToDevice));
+  // copies from pageable memory may return before their DMA ends; searches read these
+  // tables from non-blocking streams
+  ADS_CUDA(cudaDeviceSynchronize());
   *out = guard.release();
   return ADS_OK;
 }

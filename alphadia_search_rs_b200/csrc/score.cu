@@ -1499,6 +1499,9 @@ int ads_lib_set_idf(AdsLib* lib, const uint32_t* counts, double total_fragments,
     std::lock_guard<std::mutex> lk(lib->mu);
     ADS_CUDA(cudaMemcpy(lib->idf_counts.p, counts, (size_t)g.n * 4,
                         location == ADS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice));
+    // neither a pageable upload nor a device-to-device copy waits for its DMA, and the
+    // scoring kernels read the histogram from other streams
+    ADS_CUDA(cudaDeviceSynchronize());
     lib->idf_total = (float)total_fragments;  // usize as f32, as the reference converts
     return ADS_OK;
   });

@@ -352,6 +352,10 @@ __global__ void __launch_bounds__(kPrepThreads, 8) prep_kernel(PrepArgs a) {
 // unrolled stencils for the half widths of kernel_size 20, 21-22 and 31-32, any
 // other half width through the generic path.
 constexpr int kLaneCycles[] = {4, 8, 10, 12, 16};
+constexpr int kGrowLaneCycles = 16;  // cycles per lane of long-window (GROW) launches
+// Global working sets of one long-window launch: at most this many bytes (the grid
+// is trimmed to fit; a warp's set is about 15 bytes per cycle of the longest window).
+constexpr int64_t kGrowBudgetBytes = int64_t(1) << 30;
 constexpr int kDefaultWarpsPerBlock = 4;
 constexpr int kMaxClasses = 10;
 constexpr int kStats = 7;  // statistics-pass counters (ads_selection_last_stats)
@@ -383,18 +387,23 @@ int best_lane_cycles(int64_t c) {
 
 // Length classes: every bound 32 * S * k (k <= 4 passes) below the longest window, at
 // least 20 % apart, each with its cheapest lane width, then one class for the rest.
-// A fixed cycles_per_lane gives a single class.
+// A fixed cycles_per_lane gives a single class.  Windows longer than kSmemMaxCycles
+// get a class of their own, searched with the warps' working sets in global memory
+// (GROW, kGrowLaneCycles cycles per lane); everything up to kSmemMaxCycles then stays
+// in shared-memory classes.
 int plan_classes(int64_t c_max, int fixed_S, LenClasses* out) {
   int n = 0;
+  const bool grow = c_max > kSmemMaxCycles;
+  const int64_t c_sm = std::min<int64_t>(c_max, kSmemMaxCycles);
   if (fixed_S == 0) {
     std::vector<int> bounds;
     for (int S : kLaneCycles)
       for (int k = 1; k <= 4; ++k)
-        if ((int64_t)32 * S * k < c_max) bounds.push_back(32 * S * k);
+        if ((int64_t)32 * S * k < c_sm) bounds.push_back(32 * S * k);
     std::sort(bounds.begin(), bounds.end());
     int last = 0;
     for (int b : bounds) {
-      if (n == kMaxClasses - 1) break;
+      if (n == kMaxClasses - 1 - (grow ? 1 : 0)) break;
       if (last > 0 && (int64_t)b * 5 < (int64_t)last * 6) continue;
       out->bound[n] = b;
       out->S[n] = best_lane_cycles(b);
@@ -402,35 +411,51 @@ int plan_classes(int64_t c_max, int fixed_S, LenClasses* out) {
       ++n;
     }
   }
+  if (grow) {
+    out->bound[n] = kSmemMaxCycles;
+    out->S[n] = fixed_S ? fixed_S : best_lane_cycles(kSmemMaxCycles);
+    ++n;
+    out->bound[n] = (int)c_max;
+    out->S[n] = kGrowLaneCycles;
+    return n + 1;
+  }
   out->bound[n] = (int)c_max;
   out->S[n] = fixed_S ? fixed_S : best_lane_cycles(c_max);
   return n + 1;
 }
 
 template <int H, bool FAST>
-void (*pick_for_h(int S))(SearchArgs) {
+void (*pick_for_h(int S, bool grow))(SearchArgs) {
+  if (grow) return search_kernel<H, kGrowLaneCycles, FAST, true>;
   switch (S) {
-    case 4: return search_kernel<H, 4, FAST>;
-    case 8: return search_kernel<H, 8, FAST>;
-    case 10: return search_kernel<H, 10, FAST>;
-    case 12: return search_kernel<H, 12, FAST>;
-    default: return search_kernel<H, 16, FAST>;
+    case 4: return search_kernel<H, 4, FAST, false>;
+    case 8: return search_kernel<H, 8, FAST, false>;
+    case 10: return search_kernel<H, 10, FAST, false>;
+    case 12: return search_kernel<H, 12, FAST, false>;
+    default: return search_kernel<H, 16, FAST, false>;
   }
 }
 
 template <bool FAST>
-void (*pick_for_precision(int h, int S))(SearchArgs) {
+void (*pick_for_precision(int h, int S, bool grow))(SearchArgs) {
   switch (h) {
-    case 10: return pick_for_h<10, FAST>(S);
-    case 11: return pick_for_h<11, FAST>(S);
-    case 16: return pick_for_h<16, FAST>(S);
-    default: return pick_for_h<0, FAST>(S);
+    case 10: return pick_for_h<10, FAST>(S, grow);
+    case 11: return pick_for_h<11, FAST>(S, grow);
+    case 16: return pick_for_h<16, FAST>(S, grow);
+    default: return pick_for_h<0, FAST>(S, grow);
   }
 }
 
-// fast: BF16 intensity storage with the fast f32 arithmetic (ADS_PRECISION_BF16)
-void (*pick_search_kernel(int h, int S, bool fast))(SearchArgs) {
-  return fast ? pick_for_precision<true>(h, S) : pick_for_precision<false>(h, S);
+// fast: BF16 intensity storage with the fast f32 arithmetic (ADS_PRECISION_BF16);
+// grow: working sets in global memory (long windows; S must be kGrowLaneCycles)
+void (*pick_search_kernel(int h, int S, bool fast, bool grow))(SearchArgs) {
+  return fast ? pick_for_precision<true>(h, S, grow) : pick_for_precision<false>(h, S, grow);
+}
+
+// Long-window launches: blocks whose working sets fit kGrowBudgetBytes (at least one).
+int64_t grow_blocks(int64_t blocks, int nw, size_t warp_bytes, size_t budget) {
+  const int64_t fit = (int64_t)(budget / std::max<size_t>(warp_bytes, 1)) / nw;
+  return std::max<int64_t>(1, std::min(blocks, fit));
 }
 
 // Kernel taps w[0..h] of a launch, also each twice as one packed f32x2 operand,
@@ -565,6 +590,7 @@ struct AdsSelection {
   ads::DevBuf<unsigned long long> work;
   ads::DevBuf<int> class_lists;
   ads::DevBuf<int64_t> block_sums;
+  ads::DevBuf<float> grow;  // warps' working sets of long-window launches
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // one set of four events per timed search since the last read-out
   std::vector<std::array<cudaEvent_t, 4>> stage_pool;
@@ -711,9 +737,6 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
 
   const float tol_max = l->has_tol ? std::max(l->max_tol, 0.0f) : prm.rt_tolerance;
   const int64_t c_max = std::max<int64_t>(1, max_cycle_span(d->rt, d->delta_t, tol_max, prm.kernel_size));
-  if (c_max > kMaxCycles)
-    return fail(ADS_ERR_INVALID_ARGUMENT, "RT windows longer than 2048 cycles are not supported (" +
-                                              std::to_string(c_max) + " cycles)");
   // length classes and their cycles per lane (a fixed cycles_per_lane: one class)
   const int S_fixed = s->o.cycles_per_lane;
   if (S_fixed != 0 &&
@@ -876,14 +899,15 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     const int ncell_b = (cmax_b + 32 * S - 1) / (32 * S) * 32 * S;
     // block shape: warps per block (one precursor per warp at a time); 4 by default,
     // which packs long-window classes into shared memory better than 8
+    const bool grow = cmax_b > kSmemMaxCycles;
     int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : kDefaultWarpsPerBlock;
     nw = std::max(1, std::min(nw, 8));
-    while (nw > 1 && search_smem_bytes(nw, S, s->h, ncell_b) > (size_t)max_smem) --nw;
-    const size_t smem = search_smem_bytes(nw, S, s->h, ncell_b);
+    while (nw > 1 && search_smem_bytes(nw, S, s->h, ncell_b, grow) > (size_t)max_smem) --nw;
+    const size_t smem = search_smem_bytes(nw, S, s->h, ncell_b, grow);
     if (smem > (size_t)max_smem)
-      return fail(ADS_ERR_INVALID_ARGUMENT, "RT window too long for shared memory (" +
-                                                std::to_string(c_max) + " cycles)");
-    void (*kern)(SearchArgs) = pick_search_kernel(s->h, S, bf16);
+      return fail(ADS_ERR_INTERNAL, "search kernel plan exceeds shared memory (" +
+                                        std::to_string(cmax_b) + " cycles)");
+    void (*kern)(SearchArgs) = pick_search_kernel(s->h, S, bf16, grow);
     ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
     ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
@@ -894,7 +918,14 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     sa.c_max = cmax_b;
     sa.ncell = ncell_b;
     sa.work = s->work.p + b;
-    const int64_t blocks = std::min<int64_t>((int64_t)s->num_sms * bps, (P + nw - 1) / nw);
+    int64_t blocks = std::min<int64_t>((int64_t)s->num_sms * bps, (P + nw - 1) / nw);
+    sa.grow = nullptr;
+    if (grow) {
+      const size_t warp_bytes = (size_t)warp_plan(S, s->h, ncell_b).total * 4;
+      blocks = grow_blocks(blocks, nw, warp_bytes, (size_t)kGrowBudgetBytes);
+      ADS_TRY(s->grow.reserve((size_t)blocks * nw * warp_bytes / 4));
+      sa.grow = s->grow.p;
+    }
     kern<<<(int)blocks, nw * 32, smem, st>>>(sa);
     ADS_LAUNCH_CHECK();
     ++launches;
@@ -1023,7 +1054,7 @@ std::vector<const void*> graph_key(const AdsSelection* s, const AdsDia* d, const
   return {d, l, c, c->arena.p, s->nf.p, s->cs.p, s->ce.p, s->nwin.p, s->wins.p, s->fw.p,
           s->blo.p, s->bhi.p, s->keep.p, s->cand_n.p, s->cand_score.p, s->cand_center.p,
           s->work.p, s->class_lists.p, s->block_sums.p, s->stats_on ? s->stats.p : nullptr,
-          d->intens_bf16.p};
+          d->intens_bf16.p, s->grow.p};
 }
 
 // A search, with use_graph: the first search of a (run, library, collection) runs
@@ -1358,6 +1389,9 @@ int noalloc_scratch(int device, char** out) {
   ADS_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
   const std::vector<double2> tab = host_ln_table();
   ADS_CUDA(cudaMemcpy(p, tab.data(), kNoAllocLnBytes, cudaMemcpyHostToDevice));
+  // a copy from pageable memory may return before its DMA ends; the search kernels
+  // run on the caller's stream, which need not wait for the legacy stream
+  ADS_CUDA(cudaDeviceSynchronize());
   g_noalloc_base[device] = static_cast<char*>(p);
   *out = static_cast<char*>(p);
   return ADS_OK;
@@ -1381,6 +1415,9 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
                    float* o_score, uint64_t* o_center, uint64_t* o_start, uint64_t* o_stop,
                    int64_t* o_count, int32_t* o_flags) {
   if (!d || !l || !params || !o_count) return fail(ADS_ERR_INVALID_ARGUMENT, "null argument");
+  if (!o_flags)
+    return fail(ADS_ERR_INVALID_ARGUMENT,
+                "flags must point to a device int32: the kernels report internal errors there");
   if (d->device != l->device) return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
   std::vector<float> kernel;
   int h = 0;
@@ -1397,10 +1434,10 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   const int64_t n_rt = (int64_t)d->rt.size();
   const float tol_max = l->has_tol ? std::max(l->max_tol, 0.0f) : prm.rt_tolerance;
   const int64_t c_max = std::max<int64_t>(1, max_cycle_span(d->rt, d->delta_t, tol_max, prm.kernel_size));
-  if (c_max > kMaxCycles)
-    return fail(ADS_ERR_INVALID_ARGUMENT, "RT windows longer than 2048 cycles are not supported (" +
-                                              std::to_string(c_max) + " cycles)");
-  const int S = best_lane_cycles(c_max);
+  // windows beyond the shared-memory plan: one long-window launch whose warps'
+  // working sets are carved from the scratch
+  const bool grow = c_max > kSmemMaxCycles;
+  const int S = grow ? kGrowLaneCycles : best_lane_cycles(c_max);
   const int ncell = (int)((c_max + 32 * S - 1) / (32 * S) * 32 * S);
   const int k_out = (int)std::max<int64_t>(0, std::min<int64_t>(prm.candidate_count, maxima_cap(ncell)));
   const int kf = (int)std::max<int64_t>(1, std::min<int64_t>(prm.top_k_fragments, l->max_frag));
@@ -1436,12 +1473,24 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   auto* cand_score = sc.take<float>(P * k_out);
   auto* cand_center = sc.take<int>(P * k_out);
   auto* block_sums = sc.take<int64_t>(nb);
+  // long windows: at least one block of warps' working sets must fit after the rest
+  const int nw0 = kDefaultWarpsPerBlock;
+  const size_t grow_warp_bytes = grow ? (size_t)warp_plan(S, h, ncell).total * 4 : 0;
+  float* grow_sets = nullptr;
+  size_t grow_bytes = 0;
+  if (grow) {  // the rest of the array, which must hold one block's working sets
+    grow_sets = reinterpret_cast<float*>(sc.base + sc.off);
+    const size_t need = (size_t)nw0 * grow_warp_bytes;
+    grow_bytes = sc.off < (size_t)ADS_NOALLOC_SCRATCH_BYTES ? (size_t)ADS_NOALLOC_SCRATCH_BYTES - sc.off : 0;
+    sc.off += grow_bytes >= need ? grow_bytes : need;
+  }
   if (sc.off > (size_t)ADS_NOALLOC_SCRATCH_BYTES)
     return fail(ADS_ERR_INVALID_ARGUMENT,
                 "this search needs " + std::to_string(sc.off) + " bytes of scratch, more than the " +
                     std::to_string((size_t)ADS_NOALLOC_SCRATCH_BYTES) +
                     " of ads_select_noalloc; search the library in smaller parts");
-  int* flags = o_flags ? reinterpret_cast<int*>(o_flags) : err;
+  int* flags = reinterpret_cast<int*>(o_flags);
+  (void)err;
 
   // what must start at zero: the work counter, the error flags and the count
   ADS_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
@@ -1491,15 +1540,15 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   prep_kernel<<<(int)prep_blocks, kPrepThreads, prep_smem, st>>>(pa);
   ADS_LAUNCH_CHECK();
 
-  int nw = kDefaultWarpsPerBlock;
+  int nw = nw0;
   int max_smem = 0;
   ADS_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
-  while (nw > 1 && search_smem_bytes(nw, S, h, ncell) > (size_t)max_smem) --nw;
-  const size_t smem = search_smem_bytes(nw, S, h, ncell);
+  while (nw > 1 && search_smem_bytes(nw, S, h, ncell, grow) > (size_t)max_smem) --nw;
+  const size_t smem = search_smem_bytes(nw, S, h, ncell, grow);
   if (smem > (size_t)max_smem)
-    return fail(ADS_ERR_INVALID_ARGUMENT, "RT window too long for shared memory (" +
-                                              std::to_string(c_max) + " cycles)");
-  void (*kern)(SearchArgs) = pick_search_kernel(h, S, false);
+    return fail(ADS_ERR_INTERNAL, "search kernel plan exceeds shared memory (" +
+                                      std::to_string(c_max) + " cycles)");
+  void (*kern)(SearchArgs) = pick_search_kernel(h, S, false, grow);
   ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
@@ -1535,7 +1584,12 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   sa.cand_score = cand_score;
   sa.cand_center = cand_center;
   sa.stats = nullptr;
-  const int64_t blocks = std::min<int64_t>((int64_t)n_sms * occ, (P + nw - 1) / nw);
+  int64_t blocks = std::min<int64_t>((int64_t)n_sms * occ, (P + nw - 1) / nw);
+  sa.grow = nullptr;
+  if (grow) {
+    blocks = grow_blocks(blocks, nw, grow_warp_bytes, grow_bytes);
+    sa.grow = grow_sets;
+  }
   kern<<<(int)blocks, nw * 32, smem, st>>>(sa);
   ADS_LAUNCH_CHECK();
 

@@ -48,6 +48,7 @@ struct SearchArgs {
   int ncell;   // cycles a warp's row holds: passes * 32 * S >= c_max
   int gather_mode;
   int scan_thresh;
+  float* grow;  // per-warp working sets of a long-window launch (GROW), else null
   unsigned long long* work;
   int* err;
   int* cand_n;
@@ -63,7 +64,8 @@ struct SearchArgs {
 template <bool FAST>
 constexpr int kPrefetchChunks = FAST ? 3 : 2;
 constexpr int kBitOff = 32;         // bitmap bit of cycle c is c + kBitOff (room for -h)
-constexpr int kMaxCycles = 2048;    // longest RT window (cycles) a precursor may span
+constexpr int kSmemMaxCycles = 2048;  // longest RT window (cycles) a warp's shared-memory plan
+                                      // holds; longer windows run with GROW
 constexpr int kTouchCap = 256;      // cells a row records for clearing; beyond it the row is
                                     // zeroed whole
 
@@ -138,8 +140,8 @@ __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
   return w;
 }
 
-__host__ __device__ inline size_t search_smem_bytes(int nw, int S, int h, int ncell) {
-  return (size_t)(kBlockHeaderWords + nw * warp_plan(S, h, ncell).total) * 4;
+__host__ __device__ inline size_t search_smem_bytes(int nw, int S, int h, int ncell, bool grow = false) {
+  return (size_t)(kBlockHeaderWords + (grow ? 0 : nw * warp_plan(S, h, ncell).total)) * 4;
 }
 
 // Per-warp work counters (the statistics pass); 32 bits suffice for one warp's
@@ -489,7 +491,10 @@ __device__ __forceinline__ void warp_merge_best_first(float& v, int& i, int lane
   for (int j = 16; j > 0; j >>= 1) cmpx(v, i, j, (lane & j) == 0);
 }
 
-template <int H, int S, bool FAST>
+// GROW: the warp's working set (row, tags, bitmap, scores, lists, maxima) lives in
+// a global buffer of P.total words per warp (`a.grow`) instead of shared memory, for
+// RT windows longer than kSmemMaxCycles; the code and every operation are the same.
+template <int H, int S, bool FAST, bool GROW>
 __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
   extern __shared__ __align__(16) float smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -497,7 +502,8 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
   const WarpPlan P = warp_plan(S, h, a.ncell);
   double2* lnt = reinterpret_cast<double2*>(smem_raw);
   float* kw_s = smem_raw + kLnTableSize * 4;
-  float* wb = smem_raw + kBlockHeaderWords + warp * P.total;
+  float* wb = GROW ? a.grow + ((size_t)blockIdx.x * (blockDim.x >> 5) + warp) * (size_t)P.total
+                   : smem_raw + kBlockHeaderWords + warp * P.total;
   float* row = wb + P.row;
   uint32_t* tags = reinterpret_cast<uint32_t*>(wb + P.tags);
   uint32_t* bm = reinterpret_cast<uint32_t*>(wb + P.bm);

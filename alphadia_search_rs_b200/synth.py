@@ -2,7 +2,8 @@
 benchmark configurations (no public dataset is used or reproduced).
 
 Run layout (per cycle c): one MS1 spectrum (delta_scan_idx 0, isolation [-1, -1],
-no peaks, rt = c seconds) followed by W MS2 spectra (delta_scan_idx 1..W) with
+no peaks, rt = c * cycle_time seconds, cycle_time 1 s unless a configuration says
+otherwise) followed by W MS2 spectra (delta_scan_idx 1..W) with
 contiguous isolation windows.  Each MS2 spectrum has N random peaks (m/z uniform
 in [150, 1800], intensity log-normal(mu=8, sigma=2)) plus the planted signal.
 
@@ -12,7 +13,7 @@ the y1 filter is a no-op).  A fraction ``planted`` of the targets elutes: for
 every fragment and cycle within apex +- 4 sigma a peak is inserted at the
 fragment m/z (+ N(0, 2 ppm) jitter) into the windows holding the precursor m/z
 with intensity A * lib_int * exp(-(c - apex)^2 / (2 sigma^2)) * LogNormal(0, 0.3),
-A = 1e6, sigma = 4 cycles.  Library RT = apex + N(0, 20).  Decoys (if any) have
+A = 1e6, sigma = 4 cycles.  Library RT = (apex + N(0, 20)) * cycle_time.  Decoys (if any) have
 their fragment m/z shifted by U(-50, 50), clamped to [150, 1800].
 
 Backends: ``torch`` (on a CUDA device; used for the large configurations) and
@@ -56,6 +57,7 @@ class SynthConfig:
     planted: float = 0.6
     seed: int = 0
     precision: str = "fp32"
+    cycle_time: float = 1.0        # seconds per cycle (spectrum RT = cycle * cycle_time)
 
     @property
     def fwhm_rt(self) -> float:
@@ -91,6 +93,17 @@ CONFIGS = {
     "tiny_cfg4": SynthConfig("tiny_cfg4", 700, 6, 8.0, 400.0, 400, 400, 4, 24, (400.0, 448.0),
                              (2, 4), (30.0, 300.0), 10.0, 3.0, 31, 5, 24, decoy_fraction=0.5,
                              seed=13),
+    # long RT windows: per-precursor half-windows of 400-1100 cycles on a 2600-cycle run
+    # (length classes up to cfg2/3's 801 and cfg4's 1201 cycles, the widest shared-memory
+    # plan at 2048 cycles and windows beyond it)
+    "tiny_long": SynthConfig("tiny_long", 2600, 4, 25.0, 400.0, 200, 300, 4, 24, (400.0, 500.0),
+                             (2, 4), (400.0, 1100.0), 15.0, 2.0, 21, 3, 24, decoy_fraction=0.5,
+                             seed=15),
+    # 6000 cycles of 0.5 s searched with rt_tolerance 1000 s: every window spans about
+    # 4000 cycles
+    "long_rt": SynthConfig("long_rt", 6000, 3, 25.0, 400.0, 150, 200, 12, 12, (400.0, 475.0),
+                           (2, 3), (1000.0, 1000.0), 15.0, 2.0, 21, 3, 12, seed=16,
+                           cycle_time=0.5),
     # the benchmark configurations
     "cfg0": SynthConfig("cfg0", 1000, 8, 25.0, 400.0, 1500, 2000, 12, 12, (400.0, 600.0), (2, 3),
                         (100.0, 100.0), 15.0, 2.0, 21, 3, 12, seed=100),
@@ -265,7 +278,7 @@ def make_library(cfg: SynthConfig, backend="numpy", device="cuda:0") -> dict:
     pmz = B.f32(lo + (hi - lo) * B.rand(P))
     charge = B.randint(cfg.charge_range[0], cfg.charge_range[1] + 1, P)
     apex = B.rand(P) * (cfg.n_cycles - 1)
-    prt = B.f32(apex + RT_LIB_SIGMA * B.randn(P))
+    prt = B.f32((apex + RT_LIB_SIGMA * B.randn(P)) * cfg.cycle_time)
     is_decoy = B.rand(P) < cfg.decoy_fraction
     planted = (~is_decoy) & (B.rand(P) < cfg.planted)
     owner = B.repeat(B.arange(P), nfrag)
@@ -358,7 +371,7 @@ def make_run(cfg: SynthConfig, lib: dict, backend="numpy", device="cuda:0") -> d
     else:
         iso_lo = np.where(ms1, np.float32(-1.0), iso_lo).astype(np.float32)
         iso_hi = np.where(ms1, np.float32(-1.0), iso_hi).astype(np.float32)
-    rt = B.f32(cyc.to(B.t.float64) if backend == "torch" else cyc.astype(np.float64))
+    rt = B.f32((cyc.to(B.t.float64) if backend == "torch" else cyc.astype(np.float64)) * cfg.cycle_time)
 
     # random peaks: spectrum id of MS2 spectra only
     ms2_ids = sidx[~ms1]
@@ -463,7 +476,7 @@ def _make_run_torch_blocked(cfg: SynthConfig, lib: dict, device: str) -> dict:
     ms1 = dsi == 0
     iso_lo = wlo.to(t.float32).masked_fill(ms1, -1.0)
     iso_hi = (wlo + cfg.window_width).to(t.float32).masked_fill(ms1, -1.0)
-    rt = cyc.to(t.float64).to(t.float32)
+    rt = (cyc.to(t.float64) * cfg.cycle_time).to(t.float32)
     del sidx, wlo
 
     # planted peaks (spectrum id, m/z, intensity), all cycles at once

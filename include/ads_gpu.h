@@ -14,6 +14,10 @@
  * Threading: calls on different handles may run concurrently.  A selection handle
  * owns one CUDA stream; calls that share a selection handle must be serialised by
  * the caller.  Error text is kept per host thread (ads_last_error).
+ *
+ * Device state: per device the library keeps a memory pool, the m/z grid and a log
+ * table for the life of the process.  A cudaDeviceReset while the library is in use
+ * invalidates them and is not supported.
  */
 #ifndef ADS_GPU_H
 #define ADS_GPU_H
@@ -212,20 +216,24 @@ int ads_select_async(AdsSelection* sel, const AdsDia* dia, const AdsLib* lib,
  * Runs the search of ads_select with default engine options and writes the
  * candidates, in the same order and with the same values, into caller-owned
  * device arrays of `capacity` rows (capacity >= precursors x min(candidate_count,
- * maxima capacity)); the row count goes to the device int64 *count, the kernels'
- * internal error flags (0 = none) to the device int32 *flags when it is not NULL.
- * The scan_* columns of the reference are zero and not written.  Everything is
- * enqueued on `stream` (a cudaStream_t as integer, 0 = the legacy default stream)
- * and the call returns without waiting.
+ * maxima capacity)); the row count goes to the device int64 *count and the kernels'
+ * internal error flags (0 = none; anything else means the output is not to be
+ * trusted) to the device int32 *flags, which must not be NULL.  The scan_* columns
+ * of the reference are zero and not written.  Everything is enqueued on `stream` (a
+ * cudaStream_t as integer, 0 = the legacy default stream) and the call returns
+ * without waiting.
  *
  * Working memory is a fixed device array of ADS_NOALLOC_SCRATCH_BYTES that every
  * GPU context loading this library holds until the process exits; a search that
- * needs more (about 200 bytes per precursor with 12 fragments and 3 candidates)
- * fails with ADS_ERR_INVALID_ARGUMENT and should be split over smaller libraries.
- * The first call on a device sets the array up (looks up its device address and
- * copies a 4 KiB table into it, synchronously); make that first call before any
- * stream capture.  Calls whose work overlaps on the GPU share the array and race:
- * issue them on one stream or order them with events. */
+ * needs more (about 200 bytes per precursor with 12 fragments and 3 candidates;
+ * RT windows longer than 2048 cycles also need about 60 KB per 1000 cycles for each
+ * of at least four warps) fails with ADS_ERR_INVALID_ARGUMENT and should be split
+ * over smaller libraries.  The first call on a device sets the array up (looks up its
+ * device address and copies a 4 KiB table into it, then synchronises the device);
+ * make that first call before any stream capture.  A cudaDeviceReset after it is
+ * not supported (the address is kept for the process).  Calls whose work overlaps
+ * on the GPU share the array and race: issue them on one stream or order them with
+ * events. */
 #define ADS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 int ads_select_noalloc(const AdsDia* dia, const AdsLib* lib, const AdsSelectionParams* params,
                        int64_t stream, int64_t capacity, uint64_t* precursor_idx, uint64_t* rank,

@@ -5,11 +5,15 @@ Relative score error is taken against max(|s64|, 1e-3 * max |s64| of the
 precursor), because scores near zero are common at the RT-window edges.  Bounds:
   * top-k candidate cycles: at least 99.5% identical to the oracle's (99% on the
     few-hundred-precursor cases);
-  * scores: bfloat16 keeps 8 significant bits, so every stored intensity is within
-    u = 2^-8 relative; a convolved value of non-negative intensities is then within
-    u, each ln(c + 1) term within u (ln(1 + c) >= c / (1 + c)), and the score, a
-    positive-weighted sum of such terms, within u -- the test allows u plus f32
-    noise for the maximum, and 1e-3 for the 99th percentile.
+  * scores: the north star's bound, 1e-3 relative, holds for the 99th percentile
+    and the median, and is asserted there.  It cannot hold for the maximum:
+    bfloat16 keeps 8 significant bits, so a stored intensity may be off by up to
+    u = 2^-8 = 3.9e-3 relative (just above a power of two), and a score column fed
+    by one such entry (a noise peak, or the tail of the Gaussian kernel, where
+    ln(1 + c) ~ c) carries that error unchanged.  Conversely u bounds every score:
+    a convolved value of non-negative intensities is within u, each ln(c + 1) term
+    within u (ln(1 + c) >= c / (1 + c)), and the score, a positive-weighted sum of
+    such terms, within u.  The maximum is asserted against u (plus f32 noise).
 """
 import numpy as np
 import pytest
@@ -47,8 +51,8 @@ def compare_to_fp64(got: dict, ref: dict):
 
 
 @pytest.mark.parametrize("name,min_agree", [("tiny", 0.99), ("tiny_uneven", 0.99), ("tiny_cfg4", 0.99),
-                                            ("tiny_many", 0.99),
-                                            ("cfg0", 0.995)])
+                                            ("tiny_many", 0.99), ("tiny_long", 0.99),
+                                            ("long_rt", 0.99), ("cfg0", 0.995)])
 def test_bf16_against_fp64_oracle(name, min_agree):
     cfg, lib, run = synth.make_workload(name, "numpy")
     la = synth.library_arrays(lib)
@@ -62,6 +66,7 @@ def test_bf16_against_fp64_oracle(name, min_agree):
     assert errs.max() <= SCORE_MAX_BF16, f"{name}: max relative score error {errs.max():.2e}"
     p99 = float(np.quantile(errs, 0.99))
     assert p99 <= SCORE_P99_BF16, f"{name}: 99th percentile relative score error {p99:.2e}"
+    assert float(np.median(errs)) <= SCORE_P99_BF16
 
 
 def test_bf16_deterministic():

@@ -18,7 +18,8 @@ from _util import (RUN_KEYS, assert_candidates_equal, edge_case_workload, oracle
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module", params=["tiny", "tiny_uneven", "tiny_cfg4", "tiny_many", "cfg0"])
+@pytest.fixture(scope="module", params=["tiny", "tiny_uneven", "tiny_cfg4", "tiny_many", "cfg0",
+                                        "tiny_long", "long_rt"])
 def workload(request):
     cfg, lib, run = synth.make_workload(request.param, "numpy")
     la = synth.library_arrays(lib)
@@ -273,3 +274,4 @@ def test_many_fragments_top_k(top_k):
     ref = oracle_search(run, la, params, oracle.LOG_RN)
     assert len(ref["rank"]) > 0
     assert_candidates_equal(got, ref, exact_scores=True, where=f"top-{top_k}")
+

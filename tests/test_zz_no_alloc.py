@@ -22,7 +22,19 @@ pytestmark = pytest.mark.gpu
 OUT_COLS = ("precursor_idx", "rank", "score", "cycle_center", "cycle_start", "cycle_stop")
 
 
-def noalloc_search(dia, lib, params: dict, capacity=None):
+def output_arrays(cap: int):
+    """Caller-owned device arrays for one call (torch allocates them, not the library)."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    cols = {c: torch.empty(max(cap, 1), dtype=torch.float32 if c == "score" else torch.int64,
+                           device=dev) for c in OUT_COLS}
+    count = torch.full((1,), -7, dtype=torch.int64, device=dev)
+    flags = torch.full((1,), -7, dtype=torch.int32, device=dev)
+    return cols, count, flags
+
+
+def noalloc_search(dia, lib, params: dict, capacity=None, outputs=None, flags_ptr=None):
     """One call through the C ABI into torch-owned device arrays; returns the
     candidate columns (scan_* zero, as in the reference) and the error flags."""
     import torch
@@ -30,16 +42,12 @@ def noalloc_search(dia, lib, params: dict, capacity=None):
     prm = params_from(params)
     P = lib.num_precursors
     cap = P * prm.candidate_count if capacity is None else capacity
-    dev = torch.device("cuda", 0)
-    cols = {c: torch.empty(max(cap, 1), dtype=torch.float32 if c == "score" else torch.int64,
-                           device=dev) for c in OUT_COLS}
-    count = torch.full((1,), -7, dtype=torch.int64, device=dev)
-    flags = torch.full((1,), -7, dtype=torch.int32, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    cols, count, flags = outputs if outputs is not None else output_arrays(cap)
+    stream = torch.cuda.current_stream(torch.device("cuda", 0))
     c_params = prm._c()
     rc = F.load().ads_select_noalloc(dia._h, lib._h, C.byref(c_params), stream.cuda_stream, cap,
                                      *[cols[c].data_ptr() for c in OUT_COLS], count.data_ptr(),
-                                     flags.data_ptr())
+                                     flags.data_ptr() if flags_ptr is None else flags_ptr)
     F.check(rc)
     stream.synchronize()
     n = int(count.item())
@@ -62,7 +70,7 @@ def _check_twice(run, la, params):
         assert_candidates_equal(got, ref, exact_scores=True, where=f"call {call}")
 
 
-@pytest.mark.parametrize("name", ["tiny", "tiny_uneven", "cfg0"])
+@pytest.mark.parametrize("name", ["tiny", "tiny_uneven", "tiny_cfg4", "cfg0", "tiny_long", "long_rt"])
 def test_noalloc_matches_select(name):
     cfg, lib, run = synth.make_workload(name, "numpy")
     _check_twice(run, synth.library_arrays(lib), cfg.params_dict())
@@ -109,3 +117,50 @@ def test_noalloc_rejects_search_beyond_scratch():
         fragment_position=np.ones(NF, np.uint8), fragment_type=np.full(NF, 98, np.uint8))
     with pytest.raises(ValueError, match="scratch"):
         noalloc_search(dia, lib, cfg.params_dict())
+
+
+def test_noalloc_after_a_larger_different_search():
+    """The scratch keeps whatever the previous call left: a long-window search over a
+    larger library fills it first, then a smaller search of another run must still
+    give exactly what ads_select gives."""
+    cfg_a, lib_a, run_a = synth.make_workload("tiny_long", "numpy")
+    _, dia_a, slib_a, _ = product_search(run_a, synth.library_arrays(lib_a), cfg_a.params_dict())
+    noalloc_search(dia_a, slib_a, cfg_a.params_dict())
+    cfg_b, lib_b, run_b = synth.make_workload("tiny", "numpy")
+    ref, dia_b, slib_b, _ = product_search(run_b, synth.library_arrays(lib_b), cfg_b.params_dict())
+    got, flags = noalloc_search(dia_b, slib_b, cfg_b.params_dict())
+    assert flags == 0
+    assert_candidates_equal(got, ref, exact_scores=True, where="after a larger search")
+
+
+def test_noalloc_allocates_nothing():
+    """After its first call on the device (which looks up the scratch array), a call
+    leaves the device's free memory and torch's caching allocator untouched."""
+    import torch
+
+    cfg, lib, run = synth.make_workload("tiny_uneven", "numpy")
+    params = cfg.params_dict()
+    ref, dia, slib, _ = product_search(run, synth.library_arrays(lib), params)
+    cap = slib.num_precursors * params["candidate_count"]
+    outputs = output_arrays(cap)
+    noalloc_search(dia, slib, params, outputs=outputs)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    reserved0 = torch.cuda.memory_reserved(0)
+    F.load()  # no library calls between the two measurements but the search
+    got, flags = noalloc_search(dia, slib, params, outputs=outputs)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert torch.cuda.memory_reserved(0) == reserved0
+    assert free1 == free0, f"device free memory changed by {free0 - free1} bytes"
+    assert flags == 0
+    assert_candidates_equal(got, ref, exact_scores=True, where="allocation check")
+
+
+def test_noalloc_rejects_null_flags():
+    """The kernels report internal errors through *flags, so it may not be NULL."""
+    cfg, lib, run = synth.make_workload("tiny", "numpy")
+    params = cfg.params_dict()
+    _, dia, slib, _ = product_search(run, synth.library_arrays(lib), params)
+    with pytest.raises(ValueError, match="flags"):
+        noalloc_search(dia, slib, params, flags_ptr=0)
