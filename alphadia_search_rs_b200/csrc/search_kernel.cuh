@@ -150,15 +150,27 @@ struct Counters {
   unsigned int read = 0, acc = 0, off = 0, pairs = 0, bins1 = 0, frag = 0;
 };
 
+// Marks cell `bit` (bitmap index) touched; UNIQ: returns whether it was not yet.
+template <bool UNIQ>
+__device__ __forceinline__ bool mark_touched(uint32_t* bm, int bit) {
+  const uint32_t m = 1u << (bit & 31);
+  if (UNIQ) return (atomicOr(bm + (bit >> 5), m) & m) == 0u;
+  atomicOr(bm + (bit >> 5), m);
+  return false;
+}
+
 // The rare case of add_chunk: lanes that hit the same cycle are grouped and summed
 // by their lowest lane in lane order (kept out of line: it is seldom taken).
-static __device__ __noinline__ void add_chunk_grouped(bool inc, int cell, int addr, float v,
+// Returns, on the lane that added, what mark_touched returned.
+template <bool UNIQ>
+static __device__ __noinline__ bool add_chunk_grouped(bool inc, int cell, int addr, float v,
                                                       int lane, float* row, uint32_t* bm,
                                                       float* scr) {
   const int key = inc ? cell : (-1 - lane);
   const unsigned grp = __match_any_sync(kFull, key);
   scr[lane] = v;
   __syncwarp();
+  bool fresh = false;
   if (inc && lane == __ffs(grp) - 1) {
     float acc = row[addr];
     unsigned g = grp;
@@ -168,9 +180,9 @@ static __device__ __noinline__ void add_chunk_grouped(bool inc, int cell, int ad
       g &= g - 1;
     }
     row[addr] = acc;
-    const int bit = cell + kBitOff;
-    atomicOr(bm + (bit >> 5), 1u << (bit & 31));
+    fresh = mark_touched<UNIQ>(bm, cell + kBitOff);
   }
+  return fresh;
 }
 
 // Adds one chunk of 32 CSR-consecutive entries to the XIC row in lane order (the
@@ -178,29 +190,41 @@ static __device__ __noinline__ void add_chunk_grouped(bool inc, int cell, int ad
 // Every accepted lane writes its lane number into its cycle's tag; a lane that
 // reads back another number shares the cycle, and only then are the lanes grouped
 // and summed by their lowest lane one rounded add at a time.
-// Accepted cells are also appended to `touched` (the next row clears them).
+// Cells are recorded in `touched` for the next row to clear: every accepted entry's
+// cell, or (UNIQ) each cell once, when its first entry arrives.
+template <bool UNIQ>
 __device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v, int lane,
                                           float* row, uint32_t* bm, uint32_t* tags, float* scr,
                                           unsigned int& n_acc, uint16_t* touched, int& n_touched) {
   const unsigned act = __ballot_sync(kFull, inc);
   if (act == 0) return;
   n_acc += __popc(act);
-  if (inc) {
-    const int at = n_touched + __popc(act & ((1u << lane) - 1u));
-    if (at < kTouchCap) touched[at] = (uint16_t)cell;
+  if (!UNIQ) {
+    if (inc) {
+      const int at = n_touched + __popc(act & ((1u << lane) - 1u));
+      if (at < kTouchCap) touched[at] = (uint16_t)cell;
+    }
+    n_touched += __popc(act);
   }
-  n_touched += __popc(act);
   if (inc) tags[cell] = (uint32_t)lane;
   __syncwarp();
   const bool dup = inc && tags[cell] != (uint32_t)lane;
-  const int bit = cell + kBitOff;
+  bool fresh = false;
   if (!__any_sync(kFull, dup)) {
     if (inc) {
       row[addr] = __fadd_rn(row[addr], v);
-      atomicOr(bm + (bit >> 5), 1u << (bit & 31));
+      fresh = mark_touched<UNIQ>(bm, cell + kBitOff);
     }
   } else {
-    add_chunk_grouped(inc, cell, addr, v, lane, row, bm, scr);
+    fresh = add_chunk_grouped<UNIQ>(inc, cell, addr, v, lane, row, bm, scr);
+  }
+  if (UNIQ) {
+    const unsigned fm = __ballot_sync(kFull, fresh);
+    if (fresh) {
+      const int at = n_touched + __popc(fm & ((1u << lane) - 1u));
+      if (at < kTouchCap) touched[at] = (uint16_t)cell;
+    }
+    n_touched += __popc(fm);
   }
   __syncwarp();
 }
@@ -268,8 +292,9 @@ __device__ __forceinline__ bool scans(const SearchArgs& a, uint32_t n) {
   return a.gather_mode == 1 || (a.gather_mode == 0 && n <= (uint32_t)a.scan_thresh);
 }
 
-// `pre`: the range's first batch, already loaded (or null).
-template <int S, bool FAST>
+// `pre`: the range's first batch, already loaded (or null).  Row addresses: cell
+// c + off through raddr<S> (the exact kernel's segmented row), or (UNIQ) c itself.
+template <int S, bool FAST, bool UNIQ>
 __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64_t wbase,
                                             uint32_t b0, uint32_t b1, uint32_t rs, uint32_t re,
                                             int cs, int ce, int lane, float* row, int off,
@@ -313,8 +338,8 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
           }
         }
         const int cell = cu - cs;
-        add_chunk(inc, cell, inc ? raddr<S>(cell + off) : 0, bt.v[u], lane, row, bm, tags, scr,
-                  k.acc, touched, n_touched);
+        add_chunk<UNIQ>(inc, cell, inc ? (UNIQ ? cell : raddr<S>(cell + off)) : 0, bt.v[u], lane,
+                        row, bm, tags, scr, k.acc, touched, n_touched);
       }
     }
   } else {
@@ -356,8 +381,8 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
         const int c = vt ? (int)__ldg(cy + q) : 0;
         const float v = vt ? ld_intensity<FAST>(e, (uint32_t)q) : 0.0f;
         const int cell = c - cs;
-        add_chunk(vt, cell, vt ? raddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, k.acc,
-                  touched, n_touched);
+        add_chunk<UNIQ>(vt, cell, vt ? (UNIQ ? cell : raddr<S>(cell + off)) : 0, v, lane, row, bm,
+                        tags, scr, k.acc, touched, n_touched);
       }
     }
   }
@@ -491,6 +516,206 @@ __device__ __forceinline__ void warp_merge_best_first(float& v, int& i, int lane
   for (int j = 16; j > 0; j >>= 1) cmpx(v, i, j, (lane & j) == 0);
 }
 
+// The CSR ranges of a precursor's (fragment, window) pairs, fetched 32 at a time
+// (lane q holds pair pb + q), and the first batch of the next row's first pair,
+// loaded while the current row is convolved.
+template <bool FAST>
+struct PairCursor {
+  int pb = -64;
+  uint32_t rs = 0, re = 0, b0 = 0, b1 = 0;
+  int wsel = 0;
+  int64_t wbase = 0;
+  ScanBatch<kPrefetchChunks<FAST>> pre;
+  int pre_pi = -1;
+};
+
+// Gathers fragment f's XIC row: its (fragment, window) pairs in window order (the
+// reference's DenseXICObservation::new, src/dense_xic_observation/mod.rs:30-64),
+// then prefetches the first batch of the next fragment's first pair.
+template <int S, bool FAST, bool UNIQ>
+__device__ __forceinline__ void gather_row(const SearchArgs& a, int64_t p, int f, int nwin,
+                                           int npairs, int cs, int ce, int lane,
+                                           PairCursor<FAST>& pc, float* row, int off,
+                                           uint32_t* bm, uint32_t* tags, float* scr, Counters& k,
+                                           uint16_t* touched, int& n_touched) {
+  for (int wi = 0; wi < nwin; ++wi) {
+    const int pi = f * nwin + wi;
+    if (pi >= pc.pb + 32) {
+      pc.pb = pi;
+      const int pj = pc.pb + lane;
+      pc.rs = pc.re = 0;
+      pc.b0 = pc.b1 = 0;
+      pc.wsel = 0;
+      pc.wbase = 0;
+      if (pj < npairs) {
+        const int fj = pj / nwin, wj = pj - fj * nwin;
+        const int64_t fo = p * a.kf + fj;
+        pc.b0 = a.blo[fo];
+        pc.b1 = a.bhi[fo];
+        pc.wsel = a.wins[p * a.maxw + wj];
+        if (pc.b1 > pc.b0) {
+          const WinInfo w = a.win[pc.wsel];
+          pc.wbase = w.base;
+          pc.rs = __ldg(a.ss + w.ss_off + pc.b0);
+          pc.re = __ldg(a.ss + w.ss_off + pc.b1);
+        }
+      }
+    }
+    const int q = pi - pc.pb;
+    const uint32_t qrs = __shfl_sync(kFull, pc.rs, q);
+    const uint32_t qre = __shfl_sync(kFull, pc.re, q);
+    const uint32_t qb0 = __shfl_sync(kFull, pc.b0, q);
+    const uint32_t qb1 = __shfl_sync(kFull, pc.b1, q);
+    const int qw = __shfl_sync(kFull, pc.wsel, q);
+    const int64_t qbase = __shfl_sync(kFull, pc.wbase, q);
+    if (qb1 <= qb0) continue;
+    k.off += 2;
+    k.pairs += 1;
+    k.bins1 += qb1 - qb0 + 1;
+    gather_pair<S, FAST, UNIQ>(a, qw, qbase, qb0, qb1, qrs, qre, cs, ce, lane, row, off, bm, tags,
+                               scr, k, pi == pc.pre_pi ? &pc.pre : nullptr, touched, n_touched);
+  }
+  __syncwarp();
+  const int pn = (f + 1) * nwin;
+  pc.pre_pi = -1;
+  if (pn < npairs && pn < pc.pb + 32) {
+    const int q = pn - pc.pb;
+    const uint32_t nrs = __shfl_sync(kFull, pc.rs, q), nre = __shfl_sync(kFull, pc.re, q);
+    const uint32_t nb0 = __shfl_sync(kFull, pc.b0, q), nb1 = __shfl_sync(kFull, pc.b1, q);
+    const int64_t nbase = __shfl_sync(kFull, pc.wbase, q);
+    if (nb1 > nb0 && nre > nrs && scans(a, nre - nrs)) {
+      load_batch<FAST>(win_entries(a, nbase), nrs, nre, lane, pc.pre);
+      pc.pre_pi = pn;
+    }
+  }
+}
+
+// Strict 5-point local maxima of a precursor's scores (src/peak_group_selection/mod.rs:33-43),
+// collected in cycle order, and the top K of them by (value descending, cycle
+// ascending), the reference's stable sort (src/peak_group_selection/mod.rs:45-61),
+// written to the candidate slots.  `score` holds cycle j at xaddr<S>(j), with two
+// readable words below cycle 0 and S + 2 cycles past C.
+template <int S>
+__device__ __forceinline__ void pick_top_k(const SearchArgs& a, int64_t p, int cs, int C,
+                                           const float* score, float* mval, int* midx, int mx,
+                                           int lane) {
+  const int passes = (C + 32 * S - 1) / (32 * S);
+  // lane l's maxima of a pass go after those of lanes < l
+  int nmax = 0;
+  for (int ps = 0; ps < passes; ++ps) {
+    const int seg = ps * 32 + lane;
+    const float* sb = score + seg * (S + 1);
+    uint32_t mk = 0;
+    if (seg * S < C - 2 && seg * S + S > 2) {
+      float v[S + 4];
+#pragma unroll
+      for (int t = 0; t < S + 4; ++t) v[t] = sb[(t - 2) + floordiv(t - 2, S)];
+#pragma unroll
+      for (int m = 0; m < S; ++m) {
+        const int i = seg * S + m;
+        const bool is = i >= 2 && i < C - 2 && v[m] < v[m + 1] && v[m + 1] < v[m + 2] &&
+                        v[m + 2] > v[m + 3] && v[m + 3] > v[m + 4];
+        mk |= (uint32_t)is << m;
+      }
+    }
+    const int cnt = __popc(mk);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    int pos = nmax + incl - cnt;
+    while (mk) {
+      const int m = __ffs(mk) - 1;
+      if (pos < mx) {
+        mval[pos] = sb[m];
+        midx[pos] = seg * S + m;
+      }
+      ++pos;
+      mk &= mk - 1;
+    }
+    nmax += __shfl_sync(kFull, incl, 31);
+  }
+  __syncwarp();
+  if (nmax > mx) {  // cannot happen: maxima are at least 4 cycles apart
+    if (lane == 0) atomicOr(a.err, 4);
+    nmax = mx;
+  }
+  const int kk = min(a.k_out, nmax);
+  if (a.k_out <= 32) {
+    // the best 32 of the maxima, sorted in the lanes: chunks of 32 are sorted
+    // and merged into the running best 32
+    float bv = -INFINITY;
+    int bi = INT_MAX;
+    for (int q0 = 0; q0 < nmax; q0 += 32) {
+      float v = q0 + lane < nmax ? mval[q0 + lane] : -INFINITY;
+      int i = q0 + lane < nmax ? midx[q0 + lane] : INT_MAX;
+      warp_sort_best_first(v, i, lane);
+      if (q0 == 0) {
+        bv = v;
+        bi = i;
+      } else {
+        const float rv = __shfl_sync(kFull, v, 31 - lane);
+        const int ri = __shfl_sync(kFull, i, 31 - lane);
+        if (better(rv, ri, bv, bi)) {
+          bv = rv;
+          bi = ri;
+        }
+        warp_merge_best_first(bv, bi, lane);
+      }
+    }
+    if (lane < kk) {
+      a.cand_score[p * a.k_out + lane] = bv;
+      a.cand_center[p * a.k_out + lane] = cs + bi;
+    }
+  }
+  for (int r = 0; a.k_out > 32 && r < kk; ++r) {
+    float bv = 0.0f;
+    int bi = -1, bk = -1;
+    for (int q = lane; q < nmax; q += 32) {
+      const float v = mval[q];
+      const int i = midx[q];
+      if (v != v) continue;  // already taken
+      if (bk < 0 || v > bv || (v == bv && i < bi)) {
+        bv = v;
+        bi = i;
+        bk = q;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      const float ov = __shfl_xor_sync(kFull, bv, o);
+      const int oi = __shfl_xor_sync(kFull, bi, o);
+      const int ok = __shfl_xor_sync(kFull, bk, o);
+      if (ok >= 0 && (bk < 0 || ov > bv || (ov == bv && oi < bi))) {
+        bv = ov;
+        bi = oi;
+        bk = ok;
+      }
+    }
+    if (lane == 0) {
+      a.cand_score[p * a.k_out + r] = bv;
+      a.cand_center[p * a.k_out + r] = cs + bi;
+      mval[bk] = __int_as_float(0x7fc00000);
+    }
+    __syncwarp();
+  }
+  if (lane == 0) a.cand_n[p] = kk;
+}
+
+// Per-warp work counters to the statistics pass's totals.
+__device__ __forceinline__ void flush_counters(const SearchArgs& a, const Counters& k, int lane) {
+  if (a.stats && lane == 0) {
+    atomicAdd(a.stats + 0, (unsigned long long)k.pairs);
+    atomicAdd(a.stats + 1, (unsigned long long)k.bins1);
+    atomicAdd(a.stats + 2, (unsigned long long)k.frag);
+    atomicAdd(a.stats + 3, (unsigned long long)k.read);
+    atomicAdd(a.stats + 4, (unsigned long long)k.acc);
+    atomicAdd(a.stats + 5, (unsigned long long)k.off);
+  }
+}
+
 // GROW: the warp's working set (row, tags, bitmap, scores, lists, maxima) lives in
 // a global buffer of P.total words per warp (`a.grow`) instead of shared memory, for
 // RT windows longer than kSmemMaxCycles; the code and every operation are the same.
@@ -554,16 +779,7 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
     const float wf_lane = lane < F ? __ldg(a.fw + p * a.kf + lane) : 0.0f;
     for (int i = lane; i <= C + C / S; i += 32) score[i] = 0.0f;  // cycles [0, C) with pads
 
-    // CSR ranges of up to 32 (fragment, window) pairs, fetched together: lane q
-    // holds pair pb + q
-    int pb = -64;
-    uint32_t rs = 0, re = 0, b0 = 0, b1 = 0;
-    int wsel = 0;
-    int64_t wbase = 0;
-    // the first batch of the next fragment's first pair, loaded while this
-    // fragment's row is convolved
-    ScanBatch<kPrefetchChunks<FAST>> pre;
-    int pre_pi = -1;
+    PairCursor<FAST> pc;
     for (int f = 0; f < F; ++f) {
       // the previous row's cells (and bitmap words) back to zero
       if (n_touched > kTouchCap) {
@@ -581,58 +797,8 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
       __syncwarp();
       // ---- 1. gather: the fragment's pairs in window order
       const unsigned int acc0 = k.acc;
-      for (int wi = 0; wi < nwin; ++wi) {
-        const int pi = f * nwin + wi;
-        if (pi >= pb + 32) {
-          pb = pi;
-          const int pj = pb + lane;
-          rs = re = 0;
-          b0 = b1 = 0;
-          wsel = 0;
-          wbase = 0;
-          if (pj < npairs) {
-            const int fj = pj / nwin, wj = pj - fj * nwin;
-            const int64_t fo = p * a.kf + fj;
-            b0 = a.blo[fo];
-            b1 = a.bhi[fo];
-            wsel = a.wins[p * a.maxw + wj];
-            if (b1 > b0) {
-              const WinInfo w = a.win[wsel];
-              wbase = w.base;
-              rs = __ldg(a.ss + w.ss_off + b0);
-              re = __ldg(a.ss + w.ss_off + b1);
-            }
-          }
-        }
-        const int q = pi - pb;
-        const uint32_t qrs = __shfl_sync(kFull, rs, q);
-        const uint32_t qre = __shfl_sync(kFull, re, q);
-        const uint32_t qb0 = __shfl_sync(kFull, b0, q);
-        const uint32_t qb1 = __shfl_sync(kFull, b1, q);
-        const int qw = __shfl_sync(kFull, wsel, q);
-        const int64_t qbase = __shfl_sync(kFull, wbase, q);
-        if (qb1 <= qb0) continue;
-        k.off += 2;
-        k.pairs += 1;
-        k.bins1 += qb1 - qb0 + 1;
-        gather_pair<S, FAST>(a, qw, qbase, qb0, qb1, qrs, qre, cs, ce, lane, row, P.off, bm, tags,
-                             scr, k, pi == pre_pi ? &pre : nullptr, touched, n_touched);
-      }
-      __syncwarp();
-      {
-        const int pn = (f + 1) * nwin;
-        pre_pi = -1;
-        if (pn < npairs && pn < pb + 32) {
-          const int q = pn - pb;
-          const uint32_t nrs = __shfl_sync(kFull, rs, q), nre = __shfl_sync(kFull, re, q);
-          const uint32_t nb0 = __shfl_sync(kFull, b0, q), nb1 = __shfl_sync(kFull, b1, q);
-          const int64_t nbase = __shfl_sync(kFull, wbase, q);
-          if (nb1 > nb0 && nre > nrs && scans(a, nre - nrs)) {
-            load_batch<FAST>(win_entries(a, nbase), nrs, nre, lane, pre);
-            pre_pi = pn;
-          }
-        }
-      }
+      gather_row<S, FAST, false>(a, p, f, nwin, npairs, cs, ce, lane, pc, row, P.off, bm, tags, scr,
+                                 k, touched, n_touched);
       float wf = __shfl_sync(kFull, wf_lane, f & 31);
       if (f >= 32) wf = __ldg(a.fw + p * a.kf + f);
       if (!isfinite(wf)) {
@@ -733,118 +899,7 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
     }
     __syncwarp();
 
-    // ---- strict 5-point local maxima (src/peak_group_selection/mod.rs:33-43), kept
-    // in cycle order: per pass, lane l's maxima go after those of lanes < l
-    int nmax = 0;
-    for (int ps = 0; ps < passes; ++ps) {
-      const int seg = ps * 32 + lane;
-      const float* sb = score + seg * (S + 1);
-      uint32_t mk = 0;
-      if (seg * S < C - 2 && seg * S + S > 2) {
-        float v[S + 4];
-#pragma unroll
-        for (int t = 0; t < S + 4; ++t) v[t] = sb[(t - 2) + floordiv(t - 2, S)];
-#pragma unroll
-        for (int m = 0; m < S; ++m) {
-          const int i = seg * S + m;
-          const bool is = i >= 2 && i < C - 2 && v[m] < v[m + 1] && v[m + 1] < v[m + 2] &&
-                          v[m + 2] > v[m + 3] && v[m + 3] > v[m + 4];
-          mk |= (uint32_t)is << m;
-        }
-      }
-      const int cnt = __popc(mk);
-      int incl = cnt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t;
-      }
-      int pos = nmax + incl - cnt;
-      while (mk) {
-        const int m = __ffs(mk) - 1;
-        if (pos < P.mx) {
-          mval[pos] = sb[m];
-          midx[pos] = seg * S + m;
-        }
-        ++pos;
-        mk &= mk - 1;
-      }
-      nmax += __shfl_sync(kFull, incl, 31);
-    }
-    __syncwarp();
-    if (nmax > P.mx) {  // cannot happen: maxima are at least 4 cycles apart
-      if (lane == 0) atomicOr(a.err, 4);
-      nmax = P.mx;
-    }
-    // top-K by (value descending, cycle ascending): the reference's stable sort by
-    // value of maxima found in cycle order (src/peak_group_selection/mod.rs:45-61).
-    const int kk = min(a.k_out, nmax);
-    if (a.k_out <= 32) {
-      // the best 32 of the maxima, sorted in the lanes: chunks of 32 are sorted
-      // and merged into the running best 32
-      float bv = -INFINITY;
-      int bi = INT_MAX;
-      for (int q0 = 0; q0 < nmax; q0 += 32) {
-        float v = q0 + lane < nmax ? mval[q0 + lane] : -INFINITY;
-        int i = q0 + lane < nmax ? midx[q0 + lane] : INT_MAX;
-        warp_sort_best_first(v, i, lane);
-        if (q0 == 0) {
-          bv = v;
-          bi = i;
-        } else {
-          const float rv = __shfl_sync(kFull, v, 31 - lane);
-          const int ri = __shfl_sync(kFull, i, 31 - lane);
-          if (better(rv, ri, bv, bi)) {
-            bv = rv;
-            bi = ri;
-          }
-          warp_merge_best_first(bv, bi, lane);
-        }
-      }
-      if (lane < kk) {
-        a.cand_score[p * a.k_out + lane] = bv;
-        a.cand_center[p * a.k_out + lane] = cs + bi;
-      }
-    }
-    for (int r = 0; a.k_out > 32 && r < kk; ++r) {
-      float bv = 0.0f;
-      int bi = -1, bk = -1;
-      for (int q = lane; q < nmax; q += 32) {
-        const float v = mval[q];
-        const int i = midx[q];
-        if (v != v) continue;  // already taken
-        if (bk < 0 || v > bv || (v == bv && i < bi)) {
-          bv = v;
-          bi = i;
-          bk = q;
-        }
-      }
-#pragma unroll
-      for (int o = 16; o >= 1; o >>= 1) {
-        const float ov = __shfl_xor_sync(kFull, bv, o);
-        const int oi = __shfl_xor_sync(kFull, bi, o);
-        const int ok = __shfl_xor_sync(kFull, bk, o);
-        if (ok >= 0 && (bk < 0 || ov > bv || (ov == bv && oi < bi))) {
-          bv = ov;
-          bi = oi;
-          bk = ok;
-        }
-      }
-      if (lane == 0) {
-        a.cand_score[p * a.k_out + r] = bv;
-        a.cand_center[p * a.k_out + r] = cs + bi;
-        mval[bk] = __int_as_float(0x7fc00000);
-      }
-      __syncwarp();
-    }
-    if (lane == 0) a.cand_n[p] = kk;
+    pick_top_k<S>(a, p, cs, C, score, mval, midx, P.mx, lane);
   }
-  if (a.stats && lane == 0) {
-    atomicAdd(a.stats + 0, (unsigned long long)k.pairs);
-    atomicAdd(a.stats + 1, (unsigned long long)k.bins1);
-    atomicAdd(a.stats + 2, (unsigned long long)k.frag);
-    atomicAdd(a.stats + 3, (unsigned long long)k.read);
-    atomicAdd(a.stats + 4, (unsigned long long)k.acc);
-    atomicAdd(a.stats + 5, (unsigned long long)k.off);
-  }
+  flush_counters(a, k, lane);
 }

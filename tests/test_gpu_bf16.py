@@ -69,10 +69,49 @@ def test_bf16_against_fp64_oracle(name, min_agree):
     assert float(np.median(errs)) <= SCORE_P99_BF16
 
 
-def test_bf16_deterministic():
-    cfg, lib, run = synth.make_workload("tiny_uneven", "numpy")
+@pytest.mark.parametrize("name", ["tiny", "tiny_cfg4", "tiny_long"])
+def test_bf16_dense_stencil_against_fp64_oracle(name):
+    """The BF16 path with the exact kernel's dense stencil (fused multiply-adds) instead
+    of the scatter convolution: same accuracy bounds."""
+    cfg, lib, run = synth.make_workload(name, "numpy")
+    la = synth.library_arrays(lib)
+    got, *_ = product_search(run, la, cfg.params_dict(), precision="bf16", bf16_stencil="dense")
+    od, ol, tol = oracle_inputs(run, la)
+    ref = oracle.search(od, ol, oracle.Params(**cfg.params_dict()), rt_tolerance_per_precursor=tol,
+                        log_mode=oracle.LOG_RN, precision=1)
+    agree, errs = compare_to_fp64(got, ref)
+    assert agree >= 0.99, f"{name}: top-k cycle agreement {agree:.4f}"
+    assert errs.max() <= SCORE_MAX_BF16
+    assert float(np.quantile(errs, 0.99)) <= SCORE_P99_BF16
+
+
+@pytest.mark.parametrize("name", ["tiny_uneven", "long_rt"])
+def test_bf16_deterministic(name):
+    """XIC cells are summed in CSR order and the scatter's lanes never add to the same
+    output in one instruction, so the result does not depend on the launch shape."""
+    cfg, lib, run = synth.make_workload(name, "numpy")
     la = synth.library_arrays(lib)
     a, *_ = product_search(run, la, cfg.params_dict(), precision="bf16")
     b, *_ = product_search(run, la, cfg.params_dict(), precision="bf16", warps_per_block=2)
+    c, *_ = product_search(run, la, cfg.params_dict(), precision="bf16", warps_per_block=8)
     for k in a:
         assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+        assert np.array_equal(np.asarray(a[k]), np.asarray(c[k])), k
+
+
+def test_bf16_non_finite_library_intensity():
+    """An infinite library intensity makes every column of the score NaN (ln(1) * inf),
+    as in the FP32 path and the reference: no candidates for that precursor."""
+    from _util import edge_case_workload
+
+    run, la = edge_case_workload()
+    la = dict(la)
+    fi = np.array(la["fragment_intensity"], dtype=np.float32, copy=True)
+    fi[1] = np.inf
+    la["fragment_intensity"] = fi
+    params = dict(fwhm_rt=3.0, kernel_size=20, peak_length=5, mass_tolerance=20.0,
+                  rt_tolerance=30.0, candidate_count=3, top_k_fragments=6)
+    f32, *_ = product_search(run, la, params)
+    b16, *_ = product_search(run, la, params, precision="bf16")
+    assert set(f32["precursor_idx"].tolist()) == set(b16["precursor_idx"].tolist())
+    assert not np.isnan(b16["score"]).any()
