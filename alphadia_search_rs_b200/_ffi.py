@@ -149,6 +149,8 @@ SIGNATURES = {
                                          C.POINTER(C.c_float)]),
     # allocation-free search: dia, lib, params*, stream, capacity, six device output
     # columns, device int64 count, device int32 flags (nullable)
+    "ads_dia_device_bytes": (i64, [vp]),
+    "ads_dia_keep_bf16_only": (C.c_int, [vp]),
     "ads_select_noalloc": (C.c_int, [vp, vp, C.POINTER(AdsSelectionParams), i64, i64,
                                      vp, vp, vp, vp, vp, vp, vp, vp]),
     "ads_candidates_create": (C.c_int, [vp, C.POINTER(vp)]),

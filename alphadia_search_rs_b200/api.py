@@ -83,9 +83,17 @@ class DIAData:
     @staticmethod
     def from_arrays(spectrum_delta_scan_idx, isolation_lower_mz, isolation_upper_mz,
                     spectrum_peak_start_idx, spectrum_peak_stop_idx, spectrum_cycle_idx,
-                    spectrum_rt, peak_mz, peak_intensity, cycle, *, device: int | None = None):
+                    spectrum_rt, peak_mz, peak_intensity, cycle, *, device: int | None = None,
+                    intensity_storage: str = "f32"):
         """DIAData::from_arrays (src/dia_data/mod.rs:41-72).  The first nine arrays
-        may instead all be CUDA tensors on ``device`` (same dtypes)."""
+        may instead all be CUDA tensors on ``device`` (same dtypes).
+
+        ``intensity_storage="bf16"`` (an addition) keeps the intensities as bfloat16
+        only, for runs searched with ``precision="bf16"``: 4 instead of 6 device bytes
+        per peak; FP32 searches, scoring and quantification of such a run raise
+        ValueError."""
+        if intensity_storage not in ("f32", "bf16"):
+            raise ValueError("intensity_storage must be 'f32' or 'bf16'")
         L = _lib()
         names = ["spectrum_delta_scan_idx", "isolation_lower_mz", "isolation_upper_mz",
                  "spectrum_peak_start_idx", "spectrum_peak_stop_idx", "spectrum_cycle_idx",
@@ -133,6 +141,8 @@ class DIAData:
         d = DIAData()
         d._h = h.value
         d.device = int(dev)
+        if intensity_storage == "bf16":
+            F.check(L.ads_dia_keep_bf16_only(d._h))
         d._load_meta()
         return d
 
@@ -174,6 +184,11 @@ class DIAData:
 
     def memory_footprint_mb(self) -> float:
         return self.memory_footprint_bytes() / (1024.0 * 1024.0)
+
+    def device_bytes(self) -> int:
+        """Device memory the run holds (an addition; memory_footprint_bytes keeps the
+        reference's own accounting)."""
+        return int(_lib().ads_dia_device_bytes(self._h)) if self._h else 0
 
     @property
     def has_mobility(self) -> bool:

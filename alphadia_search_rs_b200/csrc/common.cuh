@@ -264,6 +264,7 @@ struct AdsDia {
   ads::DevBuf<uint16_t> cycles;
   ads::DevBuf<float> intens;
   ads::DevBuf<uint16_t> intens_bf16;   // built on first BF16 search
+  bool bf16_only = false;              // f32 intensities released (ads_dia_keep_bf16_only)
   int64_t n_entries = 0;
   int max_overlap = 0;                 // max number of non-empty windows covering one m/z
   std::vector<float> rt;               // MS1 retention times (RT index)

@@ -399,6 +399,12 @@ int64_t ads_dia_memory_footprint_bytes(const AdsDia* dia) {
   return total;
 }
 
+int64_t ads_dia_device_bytes(const AdsDia* dia) {
+  if (!dia) return 0;
+  return (int64_t)(dia->slice_starts.bytes() + dia->cycles.bytes() + dia->intens.bytes() +
+                   dia->intens_bf16.bytes() + dia->win_dev.bytes() + dia->rt_dev.bytes());
+}
+
 int ads_dia_rt_values(const AdsDia* dia, float* out, int64_t cap, int64_t* n) {
   return guarded([&] {
     if (!dia) return fail(ADS_ERR_INVALID_ARGUMENT, "null handle");
@@ -462,8 +468,18 @@ int ads_dia_copy_observation(const AdsDia* dia, int64_t obs, uint32_t* ss, uint1
     }
     if (cyc && n)
       ADS_CUDA(cudaMemcpy(cyc, dia->cycles.p + w.base, n * 2, cudaMemcpyDeviceToHost));
-    if (inten && n)
-      ADS_CUDA(cudaMemcpy(inten, dia->intens.p + w.base, n * 4, cudaMemcpyDeviceToHost));
+    if (inten && n) {
+      if (dia->bf16_only) {  // the stored bfloat16 values, widened
+        std::vector<uint16_t> b((size_t)n);
+        ADS_CUDA(cudaMemcpy(b.data(), dia->intens_bf16.p + w.base, n * 2, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < n; ++i) {
+          const uint32_t bits = (uint32_t)b[(size_t)i] << 16;
+          std::memcpy(inten + i, &bits, 4);
+        }
+      } else {
+        ADS_CUDA(cudaMemcpy(inten, dia->intens.p + w.base, n * 4, cudaMemcpyDeviceToHost));
+      }
+    }
     return ADS_OK;
   });
 }

@@ -979,6 +979,9 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
                  const uint64_t* pidx, const uint64_t* rank, const float* score,
                  const uint64_t* center, const uint64_t* start, const uint64_t* stop, int64_t c_max,
                  int verbose, AdsFeatures** out) {
+  if (d->bf16_only)
+    return fail(ADS_ERR_INVALID_ARGUMENT, "scoring needs the run's f32 intensities, but this run "
+                                          "keeps bfloat16 intensities only");
   if (!(p->mass_tolerance == p->mass_tolerance))
     return fail(ADS_ERR_INVALID_ARGUMENT, "mass_tolerance is NaN");
   if (p->top_k_fragments < 0) return fail(ADS_ERR_INVALID_ARGUMENT, "top_k_fragments < 0");
@@ -1091,6 +1094,9 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
 int quant_device(const AdsQuantParams* p, const AdsDia* d, AdsLib* l, int64_t n,
                  const uint64_t* pidx, const uint64_t* rank, const uint64_t* center,
                  const uint64_t* start, const uint64_t* stop, int verbose, AdsQuant** out) {
+  if (d->bf16_only)
+    return fail(ADS_ERR_INVALID_ARGUMENT, "quantification needs the run's f32 intensities, but "
+                                          "this run keeps bfloat16 intensities only");
   if (!(p->tolerance_ppm == p->tolerance_ppm))
     return fail(ADS_ERR_INVALID_ARGUMENT, "tolerance_ppm is NaN");
   if (p->top_k_fragments < 0) return fail(ADS_ERR_INVALID_ARGUMENT, "top_k_fragments < 0");

@@ -727,6 +727,14 @@ int ensure_bf16_intensities(AdsDia* d, cudaStream_t st) {
   return ADS_OK;
 }
 
+// Refusal for paths that read f32 intensities of a run that keeps bfloat16 only.
+int need_f32_intensities(const AdsDia* d, const char* what) {
+  if (!d->bf16_only) return ADS_OK;
+  return fail(ADS_ERR_INVALID_ARGUMENT,
+              std::string(what) + " needs the run's f32 intensities, but this run keeps bfloat16 "
+                                  "intensities only (built with BF16-only storage)");
+}
+
 int reserve_candidates(AdsCandidates* c, int64_t cap) {
   if (c->cap >= cap) return ADS_OK;
   const size_t n = (size_t)std::max<int64_t>(cap, 1);
@@ -776,6 +784,7 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     return fail(ADS_ERR_INVALID_ARGUMENT, "cycles_per_lane must be 0 or one of 4, 8, 10, 12, 16");
   const bool bf16 = s->o.precision == ADS_PRECISION_BF16;
   const bool sparse = bf16 && s->o.bf16_stencil == 0;
+  if (!bf16) ADS_TRY(need_f32_intensities(d, "an FP32 search"));
   LenClasses cls;
   const int n_cls = sparse ? plan_sparse_classes(c_max, &cls) : plan_classes(c_max, S_fixed, &cls);
   const int S_last = cls.S[n_cls - 1];
@@ -1386,6 +1395,22 @@ int ads_candidates_copy_out(AdsCandidates* c, uint64_t* pidx, uint64_t* rank, fl
   });
 }
 
+int ads_dia_keep_bf16_only(AdsDia* d) {
+  return guarded([&] {
+    if (!d) return fail(ADS_ERR_INVALID_ARGUMENT, "null handle");
+    DeviceGuard dg(d->device);
+    cudaStream_t st = nullptr;
+    ADS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const int rc = ensure_bf16_intensities(d, st);
+    cudaStreamDestroy(st);
+    if (rc != ADS_OK) return rc;
+    std::lock_guard<std::mutex> lk(d->mu);
+    d->intens.release();  // waits for the device to go idle first
+    d->bf16_only = true;
+    return ADS_OK;
+  });
+}
+
 int ads_candidates_destroy(AdsCandidates* c) {
   return guarded([&] {
     if (!c) return ADS_OK;
@@ -1465,6 +1490,7 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   std::vector<float> kernel;
   int h = 0;
   ADS_TRY(check_params(*params, &kernel, &h));
+  ADS_TRY(need_f32_intensities(d, "ads_select_noalloc (an FP32 search)"));
   const AdsSelectionParams& prm = *params;
   DeviceGuard dg(d->device);
   char* base = nullptr;

@@ -912,7 +912,9 @@ def run_ours(args, rank, world, local_rank):
         "launch": launch_info(head),
         "workload_stats": {"peaks": n_peaks_total, "candidates_per_step": int(head["n_cand"]),
                            "precursors_per_gpu": int(P),
-                           "resident_run_gb": dia.memory_footprint_bytes() / 1e9},
+                           "resident_run_gb": dia.device_bytes() / 1e9,
+                           "resident_run_gb_bf16_only": (dia.device_bytes() -
+                                                         4 * int(n_peaks_total)) / 1e9},
         "scoring": scoring,
         "quantification": quant,
         "clocks": clocks,

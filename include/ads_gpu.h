@@ -95,6 +95,17 @@ int ads_dia_observation_info(const AdsDia* dia, int64_t obs, float* iso_lower, f
  * cycle_indices and intensities (num_peaks entries each).  Any pointer may be NULL. */
 int ads_dia_copy_observation(const AdsDia* dia, int64_t obs, uint32_t* slice_starts,
                              uint16_t* cycle_indices, float* intensities);
+/* Bytes of device memory the run holds (CSR offsets, cycles, intensities in the
+ * stored precisions, windows, RT index).  An addition: the reference reports only
+ * its own accounting (memory_footprint_bytes). */
+int64_t ads_dia_device_bytes(const AdsDia* dia);
+/* BF16-only storage (an addition, for runs searched with ADS_PRECISION_BF16 only):
+ * rounds the intensities to bfloat16 (nearest even) once and releases the f32 array,
+ * so the run holds 4 bytes per peak (u16 cycle + bf16 intensity) instead of 6 or 8.
+ * Afterwards FP32 searches, scoring and quantification of this run fail with
+ * ADS_ERR_INVALID_ARGUMENT; BF16 searches give the same results as on the f32 run;
+ * ads_dia_copy_observation returns the stored bfloat16 values widened to f32. */
+int ads_dia_keep_bf16_only(AdsDia* dia);
 /* Length of the global 1-ppm m/z grid (src/mz_index/mod.rs:4-6,27). */
 int64_t ads_mz_grid_len(void);
 int ads_mz_grid(float* out, int64_t cap);

@@ -115,3 +115,36 @@ def test_bf16_non_finite_library_intensity():
     b16, *_ = product_search(run, la, params, precision="bf16")
     assert set(f32["precursor_idx"].tolist()) == set(b16["precursor_idx"].tolist())
     assert not np.isnan(b16["score"]).any()
+
+
+def test_bf16_only_run_storage():
+    """A run built with BF16-only intensity storage gives the same BF16 search as the
+    f32 run (the same round-to-nearest values), holds less device memory, and refuses
+    what needs f32 intensities."""
+    from alphadia_search_rs_b200 import (DIAData, PeakGroupQuantification, PeakGroupScoring,
+                                         PeakGroupSelection, QuantificationParameters,
+                                         ScoringParameters, SpecLibFlat)
+
+    from _util import COLS, RUN_KEYS, params_from
+
+    cfg, lib, run = synth.make_workload("tiny_uneven", "numpy")
+    la = synth.library_arrays(lib)
+    ref, dia32, slib, _ = product_search(run, la, cfg.params_dict(), precision="bf16")
+    dia16 = DIAData.from_arrays(*(run[k] for k in RUN_KEYS), run["cycle"], intensity_storage="bf16")
+    assert dia16.device_bytes() < dia32.device_bytes()
+    sel = PeakGroupSelection(params_from(cfg.params_dict()), verbose=False, precision="bf16")
+    cand = sel.search(dia16, slib)
+    got = dict(zip(COLS, cand.to_arrays()))
+    for k in COLS:
+        assert np.array_equal(np.asarray(got[k]).view(np.uint8), np.asarray(ref[k]).view(np.uint8)), k
+    o32, o16 = dia32.observation(1), dia16.observation(1)
+    assert np.array_equal(o32["cycle_indices"], o16["cycle_indices"])
+    bits = o32["intensities"].view(np.uint32).astype(np.int64)  # finite, so no carry into NaN
+    rne = ((bits + 0x7FFF + ((bits >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    assert np.array_equal(o16["intensities"].view(np.uint32), rne)
+    with pytest.raises(ValueError, match="bfloat16"):
+        PeakGroupSelection(params_from(cfg.params_dict()), verbose=False).search(dia16, slib)
+    with pytest.raises(ValueError, match="bfloat16"):
+        PeakGroupScoring(ScoringParameters(), verbose=False).score(dia16, slib, cand)
+    with pytest.raises(ValueError, match="bfloat16"):
+        PeakGroupQuantification(QuantificationParameters(), verbose=False).quantify(dia16, slib, cand)
