@@ -111,8 +111,6 @@ class AdsEngineOptions(C.Structure):
         ("time_stages", i32),
         ("cycles_per_lane", i32),
         ("stream", i64),
-        ("bf16_stencil", i32),
-        ("reserved", i32),
     ]
 
 

@@ -524,7 +524,7 @@ class PeakGroupSelection:
     def __init__(self, params: SelectionParameters, *, precision: str = "fp32", verbose: bool = True,
                  device: int | None = None, warps_per_block: int = 0, blocks_per_sm: int = 0,
                  gather_mode: int = 0, time_stages: bool = False, stream: int = 0,
-                 cycles_per_lane: int = 0, use_graph: bool = False, bf16_stencil: str = "scatter"):
+                 cycles_per_lane: int = 0, use_graph: bool = False):
         if not isinstance(params, SelectionParameters):
             raise TypeError("argument 'params': expected SelectionParameters")
         L = _lib()
@@ -541,7 +541,6 @@ class PeakGroupSelection:
         o.cycles_per_lane = int(cycles_per_lane)
         o.use_graph = 1 if use_graph else 0
         o.stream = int(stream)
-        o.bf16_stencil = {"scatter": 0, "dense": 1}[bf16_stencil]
         self._opts = o
         p = params._c()
         h = C.c_void_p()

@@ -347,7 +347,6 @@ __global__ void __launch_bounds__(kPrepThreads, 8) prep_kernel(PrepArgs a) {
 }
 
 #include "search_kernel.cuh"
-#include "search_kernel_sparse.cuh"
 
 // Cycles per lane the search kernel is compiled for, and its instances: fully
 // unrolled stencils for the half widths of kernel_size 20, 21-22 and 31-32, any
@@ -451,37 +450,6 @@ void (*pick_for_precision(int h, int S, bool grow))(SearchArgs) {
 // grow: working sets in global memory (long windows; S must be kGrowLaneCycles)
 void (*pick_search_kernel(int h, int S, bool fast, bool grow))(SearchArgs) {
   return fast ? pick_for_precision<true>(h, S, grow) : pick_for_precision<false>(h, S, grow);
-}
-
-// The BF16 (sparse) kernel for a half width: unrolled scatter for h = 10, 11, 16.
-void (*pick_sparse_kernel(int h, bool grow))(SearchArgs) {
-  switch (h) {
-    case 10: return grow ? search_kernel_sparse<10, true> : search_kernel_sparse<10, false>;
-    case 11: return grow ? search_kernel_sparse<11, true> : search_kernel_sparse<11, false>;
-    case 16: return grow ? search_kernel_sparse<16, true> : search_kernel_sparse<16, false>;
-    default: return grow ? search_kernel_sparse<0, true> : search_kernel_sparse<0, false>;
-  }
-}
-
-// Length classes of the sparse kernel, whose working set grows with the window (about
-// 16 bytes per cycle): bounds at multiples of kSparseCells below the longest window
-// (and below kSmemMaxCycles), then one class for the rest (GROW past kSmemMaxCycles).
-int plan_sparse_classes(int64_t c_max, LenClasses* out) {
-  int n = 0;
-  const int64_t c_sm = std::min<int64_t>(c_max, kSmemMaxCycles);
-  for (int b = kSparseCells; b < c_sm && n < kMaxClasses - 2; b += kSparseCells) {
-    out->bound[n] = b;
-    out->S[n] = kSparseS;
-    ++n;
-  }
-  if (c_max > kSmemMaxCycles) {
-    out->bound[n] = kSmemMaxCycles;
-    out->S[n] = kSparseS;
-    ++n;
-  }
-  out->bound[n] = (int)c_max;
-  out->S[n] = kSparseS;
-  return n + 1;
 }
 
 // Long-window launches: blocks whose working sets fit kGrowBudgetBytes (at least one).
@@ -783,10 +751,9 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
       std::find(std::begin(kLaneCycles), std::end(kLaneCycles), S_fixed) == std::end(kLaneCycles))
     return fail(ADS_ERR_INVALID_ARGUMENT, "cycles_per_lane must be 0 or one of 4, 8, 10, 12, 16");
   const bool bf16 = s->o.precision == ADS_PRECISION_BF16;
-  const bool sparse = bf16 && s->o.bf16_stencil == 0;
   if (!bf16) ADS_TRY(need_f32_intensities(d, "an FP32 search"));
   LenClasses cls;
-  const int n_cls = sparse ? plan_sparse_classes(c_max, &cls) : plan_classes(c_max, S_fixed, &cls);
+  const int n_cls = plan_classes(c_max, S_fixed, &cls);
   const int S_last = cls.S[n_cls - 1];
   const int ncell = (int)((c_max + 32 * S_last - 1) / (32 * S_last) * 32 * S_last);
   const int k_out = (int)std::max<int64_t>(0, std::min<int64_t>(prm.candidate_count, maxima_cap(ncell)));
@@ -944,17 +911,12 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     const bool grow = cmax_b > kSmemMaxCycles;
     int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : kDefaultWarpsPerBlock;
     nw = std::max(1, std::min(nw, 8));
-    auto smem_of = [&](int w) {
-      return sparse ? sparse_smem_bytes(w, s->h, ncell_b, grow)
-                    : search_smem_bytes(w, S, s->h, ncell_b, grow);
-    };
-    while (nw > 1 && smem_of(nw) > (size_t)max_smem) --nw;
-    const size_t smem = smem_of(nw);
+    while (nw > 1 && search_smem_bytes(nw, S, s->h, ncell_b, grow) > (size_t)max_smem) --nw;
+    const size_t smem = search_smem_bytes(nw, S, s->h, ncell_b, grow);
     if (smem > (size_t)max_smem)
       return fail(ADS_ERR_INTERNAL, "search kernel plan exceeds shared memory (" +
                                         std::to_string(cmax_b) + " cycles)");
-    void (*kern)(SearchArgs) =
-        sparse ? pick_sparse_kernel(s->h, grow) : pick_search_kernel(s->h, S, bf16, grow);
+    void (*kern)(SearchArgs) = pick_search_kernel(s->h, S, bf16, grow);
     ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
     ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
@@ -968,8 +930,7 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     int64_t blocks = std::min<int64_t>((int64_t)s->num_sms * bps, (P + nw - 1) / nw);
     sa.grow = nullptr;
     if (grow) {
-      const size_t warp_bytes =
-          (size_t)(sparse ? sparse_plan(s->h, ncell_b).total : warp_plan(S, s->h, ncell_b).total) * 4;
+      const size_t warp_bytes = (size_t)warp_plan(S, s->h, ncell_b).total * 4;
       blocks = grow_blocks(blocks, nw, warp_bytes, (size_t)kGrowBudgetBytes);
       ADS_TRY(s->grow.reserve((size_t)blocks * nw * warp_bytes / 4));
       sa.grow = s->grow.p;
@@ -1035,7 +996,7 @@ int autotune(AdsSelection* s, const AdsDia* d, const AdsLib* l, int32_t repeats,
     return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
   repeats = std::max(1, std::min<int32_t>(repeats, 100));
   const float tol_max = l->has_tol ? std::max(l->max_tol, 0.0f) : s->p.rt_tolerance;
-  const TuneKey key{s->device, s->o.precision * 2 + s->o.bf16_stencil, s->h,
+  const TuneKey key{s->device, s->o.precision, s->h,
                     max_cycle_span(d->rt, d->delta_t, tol_max, s->p.kernel_size), l->n_prec,
                     std::min<int64_t>(s->p.top_k_fragments, l->max_frag), l->n_frag};
   std::array<float, 3> best{0.0f, 0.0f, -1.0f};
@@ -1060,8 +1021,6 @@ int autotune(AdsSelection* s, const AdsDia* d, const AdsLib* l, int32_t repeats,
     for (int nw : {2, 4, 8}) {
       for (int S : {0, 4, 8, 10, 12, 16}) {
         if (S != 0 && (int64_t)32 * S * 8 < key.c_max) continue;  // more than 8 passes
-        // the BF16 scatter kernel has no lanes' cycles to choose
-        if (S != 0 && s->o.precision == ADS_PRECISION_BF16 && s->o.bf16_stencil == 0) continue;
         s->o.warps_per_block = nw;
         s->o.cycles_per_lane = S;
         rc = enqueue_search(s, d, l, &scratch, false);  // warm-up (and buffer sizing)
@@ -1217,8 +1176,6 @@ int ads_selection_create(const AdsSelectionParams* params, const AdsEngineOption
       return fail(ADS_ERR_INVALID_ARGUMENT, "precision must be ADS_PRECISION_FP32 or _BF16");
     if (s->o.gather_mode < 0 || s->o.gather_mode > 2)
       return fail(ADS_ERR_INVALID_ARGUMENT, "gather_mode must be 0, 1 or 2");
-    if (s->o.bf16_stencil < 0 || s->o.bf16_stencil > 1)
-      return fail(ADS_ERR_INVALID_ARGUMENT, "bf16_stencil must be 0 (scatter) or 1 (dense)");
     ADS_TRY(check_params(s->p, &s->kernel, &s->h));
     int n_dev = 0;
     if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {

@@ -150,27 +150,15 @@ struct Counters {
   unsigned int read = 0, acc = 0, off = 0, pairs = 0, bins1 = 0, frag = 0;
 };
 
-// Marks cell `bit` (bitmap index) touched; UNIQ: returns whether it was not yet.
-template <bool UNIQ>
-__device__ __forceinline__ bool mark_touched(uint32_t* bm, int bit) {
-  const uint32_t m = 1u << (bit & 31);
-  if (UNIQ) return (atomicOr(bm + (bit >> 5), m) & m) == 0u;
-  atomicOr(bm + (bit >> 5), m);
-  return false;
-}
-
 // The rare case of add_chunk: lanes that hit the same cycle are grouped and summed
 // by their lowest lane in lane order (kept out of line: it is seldom taken).
-// Returns, on the lane that added, what mark_touched returned.
-template <bool UNIQ>
-static __device__ __noinline__ bool add_chunk_grouped(bool inc, int cell, int addr, float v,
+static __device__ __noinline__ void add_chunk_grouped(bool inc, int cell, int addr, float v,
                                                       int lane, float* row, uint32_t* bm,
                                                       float* scr) {
   const int key = inc ? cell : (-1 - lane);
   const unsigned grp = __match_any_sync(kFull, key);
   scr[lane] = v;
   __syncwarp();
-  bool fresh = false;
   if (inc && lane == __ffs(grp) - 1) {
     float acc = row[addr];
     unsigned g = grp;
@@ -180,9 +168,9 @@ static __device__ __noinline__ bool add_chunk_grouped(bool inc, int cell, int ad
       g &= g - 1;
     }
     row[addr] = acc;
-    fresh = mark_touched<UNIQ>(bm, cell + kBitOff);
+    const int bit = cell + kBitOff;
+    atomicOr(bm + (bit >> 5), 1u << (bit & 31));
   }
-  return fresh;
 }
 
 // Adds one chunk of 32 CSR-consecutive entries to the XIC row in lane order (the
@@ -190,41 +178,29 @@ static __device__ __noinline__ bool add_chunk_grouped(bool inc, int cell, int ad
 // Every accepted lane writes its lane number into its cycle's tag; a lane that
 // reads back another number shares the cycle, and only then are the lanes grouped
 // and summed by their lowest lane one rounded add at a time.
-// Cells are recorded in `touched` for the next row to clear: every accepted entry's
-// cell, or (UNIQ) each cell once, when its first entry arrives.
-template <bool UNIQ>
+// Accepted cells are also appended to `touched` (the next row clears them).
 __device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v, int lane,
                                           float* row, uint32_t* bm, uint32_t* tags, float* scr,
                                           unsigned int& n_acc, uint16_t* touched, int& n_touched) {
   const unsigned act = __ballot_sync(kFull, inc);
   if (act == 0) return;
   n_acc += __popc(act);
-  if (!UNIQ) {
-    if (inc) {
-      const int at = n_touched + __popc(act & ((1u << lane) - 1u));
-      if (at < kTouchCap) touched[at] = (uint16_t)cell;
-    }
-    n_touched += __popc(act);
+  if (inc) {
+    const int at = n_touched + __popc(act & ((1u << lane) - 1u));
+    if (at < kTouchCap) touched[at] = (uint16_t)cell;
   }
+  n_touched += __popc(act);
   if (inc) tags[cell] = (uint32_t)lane;
   __syncwarp();
   const bool dup = inc && tags[cell] != (uint32_t)lane;
-  bool fresh = false;
+  const int bit = cell + kBitOff;
   if (!__any_sync(kFull, dup)) {
     if (inc) {
       row[addr] = __fadd_rn(row[addr], v);
-      fresh = mark_touched<UNIQ>(bm, cell + kBitOff);
+      atomicOr(bm + (bit >> 5), 1u << (bit & 31));
     }
   } else {
-    fresh = add_chunk_grouped<UNIQ>(inc, cell, addr, v, lane, row, bm, scr);
-  }
-  if (UNIQ) {
-    const unsigned fm = __ballot_sync(kFull, fresh);
-    if (fresh) {
-      const int at = n_touched + __popc(fm & ((1u << lane) - 1u));
-      if (at < kTouchCap) touched[at] = (uint16_t)cell;
-    }
-    n_touched += __popc(fm);
+    add_chunk_grouped(inc, cell, addr, v, lane, row, bm, scr);
   }
   __syncwarp();
 }
@@ -292,9 +268,8 @@ __device__ __forceinline__ bool scans(const SearchArgs& a, uint32_t n) {
   return a.gather_mode == 1 || (a.gather_mode == 0 && n <= (uint32_t)a.scan_thresh);
 }
 
-// `pre`: the range's first batch, already loaded (or null).  Row addresses: cell
-// c + off through raddr<S> (the exact kernel's segmented row), or (UNIQ) c itself.
-template <int S, bool FAST, bool UNIQ>
+// `pre`: the range's first batch, already loaded (or null).
+template <int S, bool FAST>
 __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64_t wbase,
                                             uint32_t b0, uint32_t b1, uint32_t rs, uint32_t re,
                                             int cs, int ce, int lane, float* row, int off,
@@ -338,8 +313,8 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
           }
         }
         const int cell = cu - cs;
-        add_chunk<UNIQ>(inc, cell, inc ? (UNIQ ? cell : raddr<S>(cell + off)) : 0, bt.v[u], lane,
-                        row, bm, tags, scr, k.acc, touched, n_touched);
+        add_chunk(inc, cell, inc ? raddr<S>(cell + off) : 0, bt.v[u], lane, row, bm, tags, scr,
+                  k.acc, touched, n_touched);
       }
     }
   } else {
@@ -381,8 +356,8 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
         const int c = vt ? (int)__ldg(cy + q) : 0;
         const float v = vt ? ld_intensity<FAST>(e, (uint32_t)q) : 0.0f;
         const int cell = c - cs;
-        add_chunk<UNIQ>(vt, cell, vt ? (UNIQ ? cell : raddr<S>(cell + off)) : 0, v, lane, row, bm,
-                        tags, scr, k.acc, touched, n_touched);
+        add_chunk(vt, cell, vt ? raddr<S>(cell + off) : 0, v, lane, row, bm, tags, scr, k.acc,
+                  touched, n_touched);
       }
     }
   }
@@ -532,7 +507,7 @@ struct PairCursor {
 // Gathers fragment f's XIC row: its (fragment, window) pairs in window order (the
 // reference's DenseXICObservation::new, src/dense_xic_observation/mod.rs:30-64),
 // then prefetches the first batch of the next fragment's first pair.
-template <int S, bool FAST, bool UNIQ>
+template <int S, bool FAST>
 __device__ __forceinline__ void gather_row(const SearchArgs& a, int64_t p, int f, int nwin,
                                            int npairs, int cs, int ce, int lane,
                                            PairCursor<FAST>& pc, float* row, int off,
@@ -572,8 +547,8 @@ __device__ __forceinline__ void gather_row(const SearchArgs& a, int64_t p, int f
     k.off += 2;
     k.pairs += 1;
     k.bins1 += qb1 - qb0 + 1;
-    gather_pair<S, FAST, UNIQ>(a, qw, qbase, qb0, qb1, qrs, qre, cs, ce, lane, row, off, bm, tags,
-                               scr, k, pi == pc.pre_pi ? &pc.pre : nullptr, touched, n_touched);
+    gather_pair<S, FAST>(a, qw, qbase, qb0, qb1, qrs, qre, cs, ce, lane, row, off, bm, tags, scr,
+                         k, pi == pc.pre_pi ? &pc.pre : nullptr, touched, n_touched);
   }
   __syncwarp();
   const int pn = (f + 1) * nwin;
@@ -797,8 +772,8 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
       __syncwarp();
       // ---- 1. gather: the fragment's pairs in window order
       const unsigned int acc0 = k.acc;
-      gather_row<S, FAST, false>(a, p, f, nwin, npairs, cs, ce, lane, pc, row, P.off, bm, tags, scr,
-                                 k, touched, n_touched);
+      gather_row<S, FAST>(a, p, f, nwin, npairs, cs, ce, lane, pc, row, P.off, bm, tags, scr, k,
+                          touched, n_touched);
       float wf = __shfl_sync(kFull, wf_lane, f & 31);
       if (f >= 32) wf = __ldg(a.fw + p * a.kf + f);
       if (!isfinite(wf)) {

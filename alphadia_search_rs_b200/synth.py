@@ -112,6 +112,10 @@ CONFIGS = {
     # cfg1's densities on 60 of its 300 windows (380-500 m/z): a profiling-sized case
     "cfg1_prof": SynthConfig("cfg1_prof", 3000, 60, 2.0, 380.0, 1000, 40_000, 12, 12, (380.0, 500.0),
                              (2, 3), (150.0, 150.0), 15.0, 2.0, 21, 3, 12, seed=101),
+    # cfg3's densities on 60 of its 300 windows (380-500 m/z): a profiling-sized case
+    "cfg3_prof": SynthConfig("cfg3_prof", 3000, 60, 2.0, 380.0, 1000, 100_000, 4, 24, (380.0, 500.0),
+                             (2, 4), (30.0, 400.0), 15.0, 2.0, 21, 3, 24, decoy_fraction=0.5, seed=102,
+                             precision="bf16"),
     "cfg2": SynthConfig("cfg2", 3000, 300, 2.0, 380.0, 1000, 500_000, 4, 24, (380.0, 980.0), (2, 4),
                         (30.0, 400.0), 15.0, 2.0, 21, 3, 24, decoy_fraction=0.5, seed=102),
     "cfg3": SynthConfig("cfg3", 3000, 300, 2.0, 380.0, 1000, 500_000, 4, 24, (380.0, 980.0), (2, 4),

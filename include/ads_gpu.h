@@ -185,10 +185,6 @@ typedef struct {
   int32_t cycles_per_lane; /* 0 = chosen from the longest RT window; else 4, 8, 10, 12
                               or 16 consecutive cycles per lane of the search kernel */
   int64_t stream;          /* cudaStream_t to run on, 0 = the handle's own stream */
-  int32_t bf16_stencil;    /* BF16 precision only: 0 = scatter convolution of the touched
-                              XIC cells (default), 1 = the exact kernel's dense stencil
-                              with fused multiply-adds (for comparison) */
-  int32_t reserved;
 } AdsEngineOptions;
 
 void ads_selection_params_default(AdsSelectionParams* p);

@@ -69,26 +69,10 @@ def test_bf16_against_fp64_oracle(name, min_agree):
     assert float(np.median(errs)) <= SCORE_P99_BF16
 
 
-@pytest.mark.parametrize("name", ["tiny", "tiny_cfg4", "tiny_long"])
-def test_bf16_dense_stencil_against_fp64_oracle(name):
-    """The BF16 path with the exact kernel's dense stencil (fused multiply-adds) instead
-    of the scatter convolution: same accuracy bounds."""
-    cfg, lib, run = synth.make_workload(name, "numpy")
-    la = synth.library_arrays(lib)
-    got, *_ = product_search(run, la, cfg.params_dict(), precision="bf16", bf16_stencil="dense")
-    od, ol, tol = oracle_inputs(run, la)
-    ref = oracle.search(od, ol, oracle.Params(**cfg.params_dict()), rt_tolerance_per_precursor=tol,
-                        log_mode=oracle.LOG_RN, precision=1)
-    agree, errs = compare_to_fp64(got, ref)
-    assert agree >= 0.99, f"{name}: top-k cycle agreement {agree:.4f}"
-    assert errs.max() <= SCORE_MAX_BF16
-    assert float(np.quantile(errs, 0.99)) <= SCORE_P99_BF16
-
-
 @pytest.mark.parametrize("name", ["tiny_uneven", "long_rt"])
 def test_bf16_deterministic(name):
-    """XIC cells are summed in CSR order and the scatter's lanes never add to the same
-    output in one instruction, so the result does not depend on the launch shape."""
+    """Every operation runs in a fixed order (XIC cells in CSR order, the stencil's taps,
+    scores in fragment order), so the result does not depend on the launch shape."""
     cfg, lib, run = synth.make_workload(name, "numpy")
     la = synth.library_arrays(lib)
     a, *_ = product_search(run, la, cfg.params_dict(), precision="bf16")
