@@ -51,6 +51,30 @@ def _as_np(name: str, x: Any, dtype) -> np.ndarray:
     return np.ascontiguousarray(x)
 
 
+_PINNED = None  # torch when page-locked host memory can be had, else False
+
+
+def _host_empty(n: int, dtype) -> np.ndarray:
+    """An uninitialised host array of n elements for device-to-host copies.  With torch
+    and a CUDA device it is page-locked memory from torch's caching host allocator
+    (freed blocks are reused, so steady-state calls do not pin new pages), which the
+    copy engines fill at full link speed; otherwise a plain numpy array."""
+    global _PINNED
+    if _PINNED is None:
+        try:
+            import torch
+
+            _PINNED = torch if torch.cuda.is_available() else False
+        except Exception:  # no torch: pageable numpy memory
+            _PINNED = False
+    if _PINNED is False:
+        return np.empty(n, dtype)
+    t = _PINNED
+    tdt = {np.dtype(np.uint64): t.uint64, np.dtype(np.float32): t.float32,
+           np.dtype(np.uint8): t.uint8, np.dtype(np.int64): t.int64}[np.dtype(dtype)]
+    return t.empty(n, dtype=tdt, pin_memory=True).numpy()
+
+
 def _dev_ptr(name: str, t: Any, dtype, device: int) -> int:
     import torch
 
@@ -740,9 +764,9 @@ class CandidateFeatureCollection:
         # one device-to-host copy, the feature columns are rows of one block
         n = self._n
         names = _feature_names()
-        pidx = np.empty(max(n, 1), np.uint64)
-        rank = np.empty(max(n, 1), np.uint64)
-        feats = np.empty((len(names), max(n, 1)), np.float32)
+        pidx = _host_empty(max(n, 1), np.uint64)
+        rank = _host_empty(max(n, 1), np.uint64)
+        feats = _host_empty(len(names) * max(n, 1), np.float32).reshape(len(names), max(n, 1))
         if self._h is not None and n:
             F.check(_lib().ads_features_copy_out(self._h, pidx.ctypes.data, rank.ctypes.data,
                                                  feats.ctypes.data))
@@ -878,22 +902,35 @@ class SpecLibFlatQuantified:
 
 
 class _Rows:
-    """Row indices for the pass-through gathers, moved to a CUDA device at most once."""
+    """Row indices for the pass-through gathers, moved to a CUDA device at most once.
+    Gathers from CUDA tensors are copied into page-locked host arrays without waiting;
+    finish() waits for all of them."""
 
     def __init__(self, rows: np.ndarray):
         self.rows = rows
         self._dev = {}
+        self._streams = []
 
     def take(self, src) -> np.ndarray:
-        """src[rows] for a numpy array or a CUDA tensor, as a numpy array."""
+        """src[rows] for a numpy array or a CUDA tensor, as a numpy array (valid after
+        finish())."""
         if _is_device_tensor(src):
             import torch
 
             key = src.device
             if key not in self._dev:
                 self._dev[key] = torch.from_numpy(self.rows).to(src.device, non_blocking=False)
-            return src.index_select(0, self._dev[key]).cpu().numpy()
+            sel = src.index_select(0, self._dev[key])
+            out = torch.empty(sel.shape, dtype=sel.dtype, pin_memory=True)
+            out.copy_(sel, non_blocking=True)
+            self._streams.append(torch.cuda.current_stream(src.device))
+            return out.numpy()
         return np.asarray(src)[self.rows]
+
+    def finish(self) -> None:
+        for st in set(self._streams):
+            st.synchronize()
+        self._streams.clear()
 
 
 class PeakGroupQuantification:
@@ -934,8 +971,8 @@ class PeakGroupQuantification:
             F.check(L.ads_quant_sizes(h, C.byref(n_p), C.byref(n_f)))
             P, NF = n_p.value, n_f.value
             out._kernel_ms = float(L.ads_quant_kernel_ms(h))
-            u = lambda m: np.empty(max(m, 1), np.uint64)
-            f = lambda m: np.empty(max(m, 1), np.float32)
+            u = lambda m: _host_empty(max(m, 1), np.uint64)
+            f = lambda m: _host_empty(max(m, 1), np.float32)
             pidx, prow, prank, prt, pfs, pfe = u(P), u(P), u(P), f(P), u(P), u(P)
             frow, fint, fmzo, fcorr, ferr, fpidx, frank = u(NF), f(NF), f(NF), f(NF), f(NF), u(NF), u(NF)
             if P:
@@ -959,6 +996,8 @@ class PeakGroupQuantification:
                      "position": fr.take(src["fragment_position"]), "type": fr.take(src["fragment_type"]),
                      "mz_observed": fmzo[:NF], "correlation_observed": fcorr[:NF],
                      "mass_error_observed": ferr[:NF], "precursor_idx": fpidx[:NF], "rank": frank[:NF]}
+        pr.finish()
+        fr.finish()
         for d in (out._prec, out._frag):
             for k, v in d.items():
                 d[k] = np.ascontiguousarray(v, _QUANT_DTYPES.get(k, np.float32))

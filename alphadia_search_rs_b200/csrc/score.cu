@@ -58,7 +58,6 @@ struct AdsQuant {
   uint64_t* rank_p = nullptr;
   uint64_t* frow_p = nullptr;
   float* fval_p[4] = {nullptr, nullptr, nullptr, nullptr};  // intensity, m/z, correlation, error
-  std::vector<int> nq;
   float kernel_ms = 0.0f;
   // the flat SpecLibFlatQuantified layout, assembled on the device
   ads::DevBuf<char> flat;
@@ -881,24 +880,26 @@ __global__ void quant_order_kernel(int64_t P, const uint32_t* perm, const uint64
 }
 
 // Assembles the flat layout of a quantification on the device.
-int quant_assemble(AdsQuant* r, cudaStream_t st) {
+struct KeptFragments {
+  __host__ __device__ uint64_t operator()(int k) const { return k > 0 ? (uint64_t)k : 0ull; }
+};
+struct KeptAny {
+  __host__ __device__ int operator()(int k) const { return k > 0 ? 1 : 0; }
+};
+
+// Totals of the two scans: fragments kept (out[0]) and candidates that kept any (out[1]).
+__global__ void quant_totals_kernel(int64_t n, const int* nq, const uint64_t* off, const int* pos,
+                                    int64_t* out) {
+  const int k = nq[n - 1];
+  out[0] = (int64_t)off[n - 1] + (k > 0 ? k : 0);
+  out[1] = (int64_t)pos[n - 1] + (k > 0 ? 1 : 0);
+}
+
+// d_off / d_pos: each candidate's first fragment row and its precursor row (exclusive
+// scans of the kept-fragment counts and of "kept any"), computed on the device.
+int quant_assemble(AdsQuant* r, const uint64_t* d_off, const int* d_pos, cudaStream_t st) {
   const int64_t n = r->n, P = r->n_prec, NF = r->n_frag;
   if (P == 0) return ADS_OK;
-  // offsets from the per-candidate counts (already on the host)
-  std::vector<int> pos((size_t)n, -1);
-  std::vector<uint64_t> off((size_t)n, 0);
-  {
-    int j = 0;
-    uint64_t o = 0;
-    for (int64_t q = 0; q < n; ++q) {
-      off[(size_t)q] = o;
-      const int k = r->nq[(size_t)q];
-      if (k > 0) {
-        pos[(size_t)q] = j++;
-        o += (uint64_t)k;
-      }
-    }
-  }
   size_t sort_bytes = 0;
   ADS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint64_t*)nullptr, (uint64_t*)nullptr,
                                            (uint32_t*)nullptr, (uint32_t*)nullptr, (int)P, 0, 64, st));
@@ -923,13 +924,10 @@ int quant_assemble(AdsQuant* r, cudaStream_t st) {
   r->f_pidx = reinterpret_cast<uint64_t*>(take(bF8));
   r->f_rank = reinterpret_cast<uint64_t*>(take(bF8));
   for (int k = 0; k < 4; ++k) r->f_val[k] = reinterpret_cast<float*>(take(bF4));
-  // temporaries: offsets, positions, unsorted precursor columns, permutation, sort space
-  const size_t bn8 = rnd((size_t)n * 8), bn4 = rnd((size_t)n * 4);
+  // temporaries: unsorted precursor columns, permutation, sort space
   DevBuf<char> tmp;
-  ADS_TRY(tmp.alloc(bn8 + bn4 + 6 * bP8 + bP4 + 2 * bP4 + rnd(sort_bytes)));
+  ADS_TRY(tmp.alloc(6 * bP8 + bP4 + 2 * bP4 + rnd(sort_bytes)));
   b = tmp.p;
-  uint64_t* d_off = reinterpret_cast<uint64_t*>(take(bn8));
-  int* d_pos = reinterpret_cast<int*>(take(bn4));
   uint64_t* u_idx = reinterpret_cast<uint64_t*>(take(bP8));
   uint64_t* u_row = reinterpret_cast<uint64_t*>(take(bP8));
   uint64_t* u_rank = reinterpret_cast<uint64_t*>(take(bP8));
@@ -941,8 +939,6 @@ int quant_assemble(AdsQuant* r, cudaStream_t st) {
   uint32_t* perm = reinterpret_cast<uint32_t*>(take(bP4));
   void* sort_tmp = take(rnd(sort_bytes));
   (void)u_spare;
-  ADS_CUDA(cudaMemcpyAsync(d_off, off.data(), (size_t)n * 8, cudaMemcpyHostToDevice, st));
-  ADS_CUDA(cudaMemcpyAsync(d_pos, pos.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
   const int grid = (int)std::min<int64_t>((n + 255) / 256, 4096);
   quant_flatten_kernel<<<grid, 256, 0, st>>>(
       n, r->Fm, r->nq_p, d_pos, d_off, r->pidx_p, r->rank_p, r->prow_p, r->rt_p, r->frow_p,
@@ -1214,21 +1210,39 @@ int quant_device(const AdsQuantParams* p, const AdsDia* d, AdsLib* l, int64_t n,
     quant_kernel<<<(int)((T + kScoreBlock - 1) / kScoreBlock), kScoreBlock, 0, st>>>(qa);
     ADS_LAUNCH_CHECK();
     ADS_CUDA(cudaEventRecord(ev.b, st));
-    r->nq.resize((size_t)n);
-    ADS_CUDA(cudaMemcpyAsync(r->nq.data(), r->nq_p, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    // where each candidate's rows go: exclusive scans of the kept-fragment counts
+    // and of "kept any fragment", and their totals
+    cub::TransformInputIterator<uint64_t, KeptFragments, const int*> frag_in(r->nq_p, KeptFragments());
+    cub::TransformInputIterator<int, KeptAny, const int*> prec_in(r->nq_p, KeptAny());
+    size_t b1 = 0, b2 = 0;
+    ADS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b1, frag_in, (uint64_t*)nullptr, (int)n, st));
+    ADS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b2, prec_in, (int*)nullptr, (int)n, st));
+    const size_t bo = rnd((size_t)n * 8), bpos = rnd((size_t)n * 4);
+    DevBuf<char> scan;
+    ADS_TRY(scan.alloc(bo + bpos + 256 + rnd(std::max(b1, b2))));
+    uint64_t* d_off = reinterpret_cast<uint64_t*>(scan.p);
+    int* d_pos = reinterpret_cast<int*>(scan.p + bo);
+    int64_t* d_tot = reinterpret_cast<int64_t*>(scan.p + bo + bpos);
+    void* scan_tmp = scan.p + bo + bpos + 256;
+    size_t bt = std::max(b1, b2);
+    ADS_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, bt, frag_in, d_off, (int)n, st));
+    bt = std::max(b1, b2);
+    ADS_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, bt, prec_in, d_pos, (int)n, st));
+    quant_totals_kernel<<<1, 1, 0, st>>>(n, r->nq_p, d_off, d_pos, d_tot);
+    ADS_LAUNCH_CHECK();
+    int64_t htot[2] = {0, 0};
     int herr = 0;
+    ADS_CUDA(cudaMemcpyAsync(htot, d_tot, sizeof(htot), cudaMemcpyDeviceToHost, st));
     ADS_CUDA(cudaMemcpyAsync(&herr, tmp.p + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     ADS_CUDA(cudaStreamSynchronize(st));
     if (herr & 1)
       return fail(ADS_ERR_INVALID_ARGUMENT, "candidate cycle range ends beyond the run's RT index");
     if (herr & 2) return fail(ADS_ERR_INTERNAL, "fragment count above the scratch plan");
     ADS_CUDA(cudaEventElapsedTime(&r->kernel_ms, ev.a, ev.b));
-    for (int v : r->nq) {
-      r->n_frag += v;
-      r->n_prec += v > 0;
-    }
+    r->n_frag = htot[0];
+    r->n_prec = htot[1];
     if (r->n_prec > INT_MAX) return fail(ADS_ERR_INVALID_ARGUMENT, "too many quantified precursors");
-    ADS_TRY(quant_assemble(r.get(), st));
+    ADS_TRY(quant_assemble(r.get(), d_off, d_pos, st));
   }
   if (verbose) {
     // src/peak_group_quantification/mod.rs:73-78 (the kernel's device time)
@@ -1459,7 +1473,9 @@ int ads_quant_copy_out(const AdsQuant* q, uint64_t* precursor_idx, uint64_t* pre
                 {mass_error_observed, q->f_val[3], NF * 4}, {fragment_precursor_idx, q->f_pidx, NF * 8},
                 {fragment_rank, q->f_rank, NF * 8}};
     for (const Col& c : cols)
-      if (c.dst) ADS_CUDA(cudaMemcpy(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost));
+      if (c.dst)
+        ADS_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, cudaStreamPerThread));
+    ADS_CUDA(cudaStreamSynchronize(cudaStreamPerThread));
     return ADS_OK;
   });
 }
