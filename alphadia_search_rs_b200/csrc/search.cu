@@ -31,7 +31,10 @@ namespace ads {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kMaxHalf = 31;       // kernel half width h <= 31 (2h+1 bits in a u64 mask)
+constexpr int kMaxHalf = 31;       // taps passed as kernel parameters up to this half width
+// widest Gaussian kernel accepted: a run has at most 65,536 cycles (u16 cycle indices)
+// and a kernel wider than the run yields no output anywhere
+constexpr int64_t kMaxKernelSize = 65536;
 constexpr int kPrepThreads = 256;  // 8 precursors per prep block
 constexpr int kScanBlock = 1024;
 
@@ -459,9 +462,11 @@ int64_t grow_blocks(int64_t blocks, int nw, size_t warp_bytes, size_t budget) {
 }
 
 // Kernel taps w[0..h] of a launch, also each twice as one packed f32x2 operand,
-// and the packed zeros of the exact stencil.
-void set_taps(SearchArgs* sa, const float* kernel, int h) {
-  for (int k = 0; k <= h; ++k) {
+// and the packed zeros of the exact stencil.  Taps past kMaxHalf are read from
+// `kw_dev` (device memory holding w[0..h]).
+void set_taps(SearchArgs* sa, const float* kernel, int h, const float* kw_dev) {
+  sa->kw_dev = h > kMaxHalf ? kw_dev : nullptr;
+  for (int k = 0; k <= std::min(h, kMaxHalf); ++k) {
     sa->kw[k] = kernel[k];
     uint32_t b;
     std::memcpy(&b, &kernel[k], 4);
@@ -591,6 +596,7 @@ struct AdsSelection {
   ads::DevBuf<int> class_lists;
   ads::DevBuf<int64_t> block_sums;
   ads::DevBuf<float> grow;  // warps' working sets of long-window launches
+  ads::DevBuf<float> taps;  // kernel taps on the device, for half widths past kMaxHalf
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // one set of four events per timed search since the last read-out
   std::vector<std::array<cudaEvent_t, 4>> stage_pool;
@@ -613,8 +619,9 @@ namespace {
 int check_params(const AdsSelectionParams& p, std::vector<float>* kernel, int* h) {
   if (p.kernel_size < 1)
     return fail(ADS_ERR_INVALID_ARGUMENT, "kernel_size must be >= 1 (the reference panics on 0)");
-  if (p.kernel_size > 2 * kMaxHalf)
-    return fail(ADS_ERR_INVALID_ARGUMENT, "kernel_size above 62 is not supported");
+  if (p.kernel_size > kMaxKernelSize)
+    return fail(ADS_ERR_INVALID_ARGUMENT,
+                "kernel_size above 65536 (wider than any run's 65,536 cycles) is not supported");
   if (p.peak_length < 0) return fail(ADS_ERR_INVALID_ARGUMENT, "peak_length < 0");
   if (p.candidate_count < 0) return fail(ADS_ERR_INVALID_ARGUMENT, "candidate_count < 0");
   if (p.top_k_fragments < 0) return fail(ADS_ERR_INVALID_ARGUMENT, "top_k_fragments < 0");
@@ -883,7 +890,7 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
   sa.inten = d->intens.p;
   sa.inten_bf16 = d->intens_bf16.p;
   sa.ln_tab = ln_tab;
-  set_taps(&sa, s->kernel.data(), s->h);
+  set_taps(&sa, s->kernel.data(), s->h, s->taps.p);
   sa.h = s->h;
   sa.k_out = k_out;
   sa.gather_mode = s->o.gather_mode;
@@ -903,14 +910,18 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     ++launches;
   }
   for (int b = 0; b < n_cls; ++b) {
-    const int S = cls.S[b];
+    int S = cls.S[b];
     const int cmax_b = cls.bound[b];
-    const int ncell_b = (cmax_b + 32 * S - 1) / (32 * S) * 32 * S;
     // block shape: warps per block (one precursor per warp at a time); 4 by default,
     // which packs long-window classes into shared memory better than 8
-    const bool grow = cmax_b > kSmemMaxCycles;
+    bool grow = cmax_b > kSmemMaxCycles;
     int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : kDefaultWarpsPerBlock;
     nw = std::max(1, std::min(nw, 8));
+    if (!grow && search_smem_bytes(1, S, s->h, (cmax_b + 32 * S - 1) / (32 * S) * 32 * S, false) >
+                     (size_t)max_smem)
+      grow = true;  // a very wide kernel: even one warp's plan exceeds shared memory
+    if (grow) S = kGrowLaneCycles;
+    const int ncell_b = (cmax_b + 32 * S - 1) / (32 * S) * 32 * S;
     while (nw > 1 && search_smem_bytes(nw, S, s->h, ncell_b, grow) > (size_t)max_smem) --nw;
     const size_t smem = search_smem_bytes(nw, S, s->h, ncell_b, grow);
     if (smem > (size_t)max_smem)
@@ -1194,6 +1205,11 @@ int ads_selection_create(const AdsSelectionParams* params, const AdsEngineOption
     }
     ADS_CUDA(cudaEventCreate(&s->ev0));
     ADS_CUDA(cudaEventCreate(&s->ev1));
+    if (s->h > kMaxHalf) {  // wide kernels: taps from device memory
+      ADS_TRY(s->taps.alloc(s->kernel.size()));
+      ADS_CUDA(cudaMemcpy(s->taps.p, s->kernel.data(), s->kernel.size() * 4, cudaMemcpyHostToDevice));
+      ADS_CUDA(cudaDeviceSynchronize());  // the upload has landed before any search reads it
+    }
     *out = s.release();
     return ADS_OK;
   });
@@ -1460,10 +1476,15 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   const int64_t n_rt = (int64_t)d->rt.size();
   const float tol_max = l->has_tol ? std::max(l->max_tol, 0.0f) : prm.rt_tolerance;
   const int64_t c_max = std::max<int64_t>(1, max_cycle_span(d->rt, d->delta_t, tol_max, prm.kernel_size));
-  // windows beyond the shared-memory plan: one long-window launch whose warps'
-  // working sets are carved from the scratch
-  const bool grow = c_max > kSmemMaxCycles;
-  const int S = grow ? kGrowLaneCycles : best_lane_cycles(c_max);
+  // windows beyond the shared-memory plan (or a kernel too wide for it): one
+  // long-window launch whose warps' working sets are carved from the scratch
+  int max_smem = 0;
+  ADS_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
+  const int S0 = best_lane_cycles(c_max);
+  const bool grow =
+      c_max > kSmemMaxCycles ||
+      search_smem_bytes(1, S0, h, (int)((c_max + 32 * S0 - 1) / (32 * S0) * 32 * S0)) > (size_t)max_smem;
+  const int S = grow ? kGrowLaneCycles : S0;
   const int ncell = (int)((c_max + 32 * S - 1) / (32 * S) * 32 * S);
   const int k_out = (int)std::max<int64_t>(0, std::min<int64_t>(prm.candidate_count, maxima_cap(ncell)));
   const int kf = (int)std::max<int64_t>(1, std::min<int64_t>(prm.top_k_fragments, l->max_frag));
@@ -1499,6 +1520,7 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   auto* cand_score = sc.take<float>(P * k_out);
   auto* cand_center = sc.take<int>(P * k_out);
   auto* block_sums = sc.take<int64_t>(nb);
+  float* taps = h > kMaxHalf ? sc.take<float>(L) : nullptr;  // wide kernels: taps on the device
   // long windows: at least one block of warps' working sets must fit after the rest
   const int nw0 = kDefaultWarpsPerBlock;
   const size_t grow_warp_bytes = grow ? (size_t)warp_plan(S, h, ncell).total * 4 : 0;
@@ -1567,8 +1589,6 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   ADS_LAUNCH_CHECK();
 
   int nw = nw0;
-  int max_smem = 0;
-  ADS_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
   while (nw > 1 && search_smem_bytes(nw, S, h, ncell, grow) > (size_t)max_smem) --nw;
   const size_t smem = search_smem_bytes(nw, S, h, ncell, grow);
   if (smem > (size_t)max_smem)
@@ -1597,7 +1617,9 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   sa.cyc = d->cycles.p;
   sa.inten = d->intens.p;
   sa.ln_tab = reinterpret_cast<const double2*>(base);
-  set_taps(&sa, kernel.data(), h);
+  if (taps)  // from pageable memory: returns once the bytes are staged, ordered on `st`
+    ADS_CUDA(cudaMemcpyAsync(taps, kernel.data(), (size_t)L * 4, cudaMemcpyHostToDevice, st));
+  set_taps(&sa, kernel.data(), h, taps);
   sa.h = h;
   sa.k_out = k_out;
   sa.c_max = (int)c_max;

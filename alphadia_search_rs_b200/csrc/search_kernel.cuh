@@ -38,7 +38,8 @@ struct SearchArgs {
   const float* inten;
   const uint16_t* inten_bf16;  // bfloat16 copy of `inten` (BF16-storage searches)
   const double2* ln_tab;
-  float kw[kMaxHalf + 1];  // kernel taps w[0..h]; w[h] is the centre
+  float kw[kMaxHalf + 1];  // kernel taps w[0..h]; w[h] is the centre (h <= kMaxHalf)
+  const float* kw_dev;     // the taps in device memory when h > kMaxHalf, else null
   unsigned long long kw2[kMaxHalf + 1];  // the same taps, each twice (packed f32x2 operands)
   unsigned long long zero2;   // +0.0f twice
   unsigned long long nzero2;  // -0.0f twice
@@ -99,15 +100,19 @@ __host__ __device__ constexpr int floordiv(int a, int b) {
 }
 
 // Per-warp shared-memory plan, in 4-byte words.  The block's ln table (double2 x
-// 256 = 1024 words) and kernel taps (32 words) come first.
+// 256 = 1024 words) and kernel taps (h + 1 words, at least 32) come first.
 struct WarpPlan {
   int row, tags, bm, scr, score, lst, mval, midx, touched, total;
   int off;        // stored index of cycle c is c + off (off >= h, a multiple of S)
   int row_words;  // words of the row, a multiple of 4
-  int bw;         // bitmap words
+  int lead;       // bitmap words below bm[0]: a window reaching h cycles before cycle 0
+                  // reads them (always zero)
+  int bw;         // bitmap words from bm[0]
   int mx;         // maxima capacity
 };
-constexpr int kBlockHeaderWords = kLnTableSize * 4 + 32;
+__host__ __device__ inline int block_header_words(int h) {
+  return kLnTableSize * 4 + ((h + 1 + 31) / 32) * 32;
+}
 
 __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
   WarpPlan w;
@@ -119,9 +124,10 @@ __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
   o += w.row_words;
   w.tags = o;
   o += ncell;
-  w.bw = (ncell + 2 * kBitOff + 32) / 32 + 2;
-  w.bm = o;
-  o += w.bw;
+  w.lead = h > kBitOff ? (h - kBitOff + 31) / 32 : 0;
+  w.bw = (ncell + h + kBitOff + 31) / 32 + 2;
+  w.bm = o + w.lead;
+  o += w.lead + w.bw;
   w.scr = o;
   o += 32;
   w.touched = o;  // cells written by the current row (16 bits each)
@@ -141,7 +147,7 @@ __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
 }
 
 __host__ __device__ inline size_t search_smem_bytes(int nw, int S, int h, int ncell, bool grow = false) {
-  return (size_t)(kBlockHeaderWords + (grow ? 0 : nw * warp_plan(S, h, ncell).total)) * 4;
+  return (size_t)(block_header_words(h) + (grow ? 0 : nw * warp_plan(S, h, ncell).total)) * 4;
 }
 
 // Per-warp work counters (the statistics pass); 32 bits suffice for one warp's
@@ -363,7 +369,9 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
   }
 }
 
-// Any bit set in bm[lo, lo + n)?  (lo >= 0, n >= 1)
+// Any bit set in bm[lo, lo + n)?  (n >= 1; lo may be negative: the shift and mask
+// below are floor division and remainder on two's-complement ints, and the words
+// below bm[0] that such a range reaches are reserved and zero)
 __device__ __forceinline__ bool bits_any(const uint32_t* bm, int lo, int n) {
   const int last = lo + n - 1;
   const int w0 = lo >> 5, w1 = last >> 5;
@@ -703,7 +711,7 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
   double2* lnt = reinterpret_cast<double2*>(smem_raw);
   float* kw_s = smem_raw + kLnTableSize * 4;
   float* wb = GROW ? a.grow + ((size_t)blockIdx.x * (blockDim.x >> 5) + warp) * (size_t)P.total
-                   : smem_raw + kBlockHeaderWords + warp * P.total;
+                   : smem_raw + block_header_words(h) + warp * P.total;
   float* row = wb + P.row;
   uint32_t* tags = reinterpret_cast<uint32_t*>(wb + P.tags);
   uint32_t* bm = reinterpret_cast<uint32_t*>(wb + P.bm);
@@ -716,11 +724,11 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
   {
     float4* r4 = reinterpret_cast<float4*>(row);
     for (int i = lane; i < P.row_words / 4; i += 32) r4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = lane; i < P.bw; i += 32) bm[i] = 0u;
+    for (int i = lane - P.lead; i < P.bw; i += 32) bm[i] = 0u;
   }
 
   for (int i = threadIdx.x; i < kLnTableSize; i += blockDim.x) lnt[i] = a.ln_tab[i];
-  for (int i = threadIdx.x; i <= a.h; i += blockDim.x) kw_s[i] = a.kw[i];
+  for (int i = threadIdx.x; i <= a.h; i += blockDim.x) kw_s[i] = a.kw_dev ? a.kw_dev[i] : a.kw[i];
   __syncthreads();
   Counters k;
 

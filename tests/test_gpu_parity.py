@@ -121,7 +121,10 @@ def test_search_deterministic(workload):
     dict(),
     dict(peak_length=15),              # center - peak_length wraps as usize
     dict(kernel_size=9, fwhm_rt=2.0),
-    dict(kernel_size=62),              # largest supported kernel
+    dict(kernel_size=62),              # widest kernel with taps in kernel parameters
+    dict(kernel_size=63),              # taps from device memory, bitmap read below cycle 0
+    dict(kernel_size=70, fwhm_rt=12.0),
+    dict(kernel_size=101),             # wider than the run: no output anywhere
     dict(kernel_size=21),              # unrolled stencil, half width 11
     dict(kernel_size=31, fwhm_rt=7.0), # unrolled stencil, half width 16
     dict(kernel_size=14),              # generic stencil, half width 7
@@ -275,3 +278,17 @@ def test_many_fragments_top_k(top_k):
     assert len(ref["rank"]) > 0
     assert_candidates_equal(got, ref, exact_scores=True, where=f"top-{top_k}")
 
+
+
+@pytest.mark.parametrize("kernel_size,fwhm_rt", [(63, 10.0), (128, 30.0), (301, 60.0)])
+def test_wide_kernels(kernel_size, fwhm_rt):
+    """Gaussian kernels wider than 62 (the reference accepts any width,
+    src/kernel/mod.rs:13-30) on windows of up to 2300 cycles: bit-exact against the
+    oracle, in shared-memory and global-memory classes."""
+    cfg, lib, run = synth.make_workload("tiny_long", "numpy")
+    la = synth.library_arrays(lib)
+    params = dict(cfg.params_dict(), kernel_size=kernel_size, fwhm_rt=fwhm_rt)
+    got, *_ = product_search(run, la, params)
+    ref = oracle_search(run, la, params, oracle.LOG_RN)
+    assert len(ref["rank"]) > 0
+    assert_candidates_equal(got, ref, exact_scores=True, where=f"kernel_size {kernel_size}")

@@ -83,6 +83,12 @@ def test_noalloc_matches_select_edge_cases():
     _check_twice(run, la, params)
 
 
+def test_noalloc_matches_select_wide_kernel():
+    """A kernel wider than 62: its taps go into the scratch array too."""
+    cfg, lib, run = synth.make_workload("tiny_long", "numpy")
+    _check_twice(run, synth.library_arrays(lib), dict(cfg.params_dict(), kernel_size=128, fwhm_rt=30.0))
+
+
 def test_noalloc_rejects_small_capacity():
     cfg, lib, run = synth.make_workload("tiny", "numpy")
     params = cfg.params_dict()
