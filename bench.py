@@ -500,16 +500,18 @@ def cpu_model() -> str:
     return "unknown"
 
 
-def load_traffic(name: str):
-    """Per-launch DRAM bytes of the search kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", f"search_kernel_{name}.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                if line.strip().startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1].strip())
-    except OSError:
-        pass
+def load_traffic(name: str, precision: str):
+    """DRAM bytes of one search's search_kernel launches (all length classes) for this
+    workload and precision, from the committed ncu summary (profiles/), or None."""
+    key = f"traffic_bytes_per_search_{precision}:"
+    for fname in (f"search_kernel_{name}_prof.md", f"search_kernel_{name}.md"):
+        try:
+            with open(os.path.join(ROOT, "profiles", fname)) as f:
+                for line in f:
+                    if line.strip().startswith(key):
+                        return float(line.split(":", 1)[1].strip())
+        except OSError:
+            pass
     return None
 
 
@@ -715,6 +717,10 @@ def search_roofline(stats, stages, precision, kernel, P, nf_raw, n_cand, ms_per_
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
             "kernel": "search_kernel", "bytes_per_intensity": s_i,
+            "launch_unit": "one search: the search_kernel launches of its RT-window length "
+                           "classes together (per_launch fields are per search)",
+            "traffic_source": "ncu DRAM bytes of a profiling-sized case at the same densities, "
+                              "scaled by the precursor count (profiles/)",
             "algorithmic_bytes_per_launch": gather_bytes,
             "kernel_ms_per_launch": search_ms,
             "path_bytes_per_step": path_bytes,
@@ -823,7 +829,7 @@ def run_ours(args, rank, world, local_rank):
     roof = {prec: search_roofline(stats, timed[prec]["stages"], prec, timed[prec]["kernel"], P, nf_raw,
                                   timed[prec]["n_cand"], timed[prec]["ms"] / args.steps, peak, peak_kind,
                                   clocks.get("sm_max_mhz"),
-                                  load_traffic(f"{cfg.name}_{prec}") or load_traffic(cfg.name))
+                                  load_traffic(cfg.name, prec))
             for prec in arms}
 
     # ---- CPU baseline (oracle port on the host cores, bounded sample) and the

@@ -42,3 +42,17 @@ def test_bf16_agreement_floors_the_denominator_near_zero():
     agree, errs = bench.bf16_agreement(got, ref)
     assert agree == 1.0
     assert abs(max(errs) - (1e-4 - 1e-9) / 1e-2) < 1e-9
+
+
+def test_traffic_comes_from_the_committed_profiles():
+    # DRAM bytes of one search's search_kernel launches, per workload and precision
+    assert bench.load_traffic("cfg3", "bf16") > bench.load_traffic("cfg3", "fp32") * 0.5
+    assert bench.load_traffic("cfg1", "fp32") > 0
+    assert bench.load_traffic("cfg1", "bf16") is None
+
+
+def test_both_arms_print_the_same_config():
+    cfg = synth.get_config("cfg3")
+    a = bench.bench_config(cfg, "bf16", 1)
+    assert a == bench.bench_config(cfg, "bf16", 1)
+    assert a["workload"].startswith("cfg3") and "per precursor" in a["rt_tolerance"]
