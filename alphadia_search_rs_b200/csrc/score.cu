@@ -118,6 +118,10 @@ struct ScoreArgs {
   float* o_feat;
   uint8_t* o_found;
   int* err;
+  // nullable: the order in which the threads take the candidates (by their precursor's
+  // library fragment count, so that the threads of a warp do similar work); results
+  // are written at each candidate's own index either way
+  const uint32_t* order;
 };
 
 // Words of one thread's scratch.
@@ -346,6 +350,56 @@ __device__ uint32_t longest_series(const Scr& s, int64_t etype, int64_t enum_, i
   return mx;
 }
 
+// Sort key of each candidate for the work order: its precursor's library fragment count
+// (capped at 255; 0 when the precursor is not in the library), and its index.
+__global__ void work_key_kernel(int64_t n, const uint64_t* c_pidx, int64_t P, const uint64_t* l_pidx,
+                                const uint64_t* l_fs, const uint64_t* l_fe, uint32_t* key,
+                                uint32_t* idx) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t x = c_pidx[q];
+    uint32_t k = 0;
+    if (P > 0) {
+      int64_t size = P, base = 0;
+      while (size > 1) {
+        const int64_t half = size / 2, mid = base + half;
+        base = l_pidx[mid] > x ? base : mid;
+        size -= half;
+      }
+      if (l_pidx[base] == x) {
+        const uint64_t nraw = l_fe[base] - l_fs[base];
+        k = nraw < 255ull ? (uint32_t)nraw : 255u;
+      }
+    }
+    key[q] = k;
+    idx[q] = (uint32_t)q;
+  }
+}
+
+// The candidates' work order (ScoreArgs::order): indices stably sorted by work_key_kernel's
+// key.  `buf` receives the order and holds the sort's temporaries.
+int work_order(int64_t n, const uint64_t* c_pidx, const AdsLib* l, cudaStream_t st, DevBuf<char>* buf,
+               const uint32_t** order) {
+  *order = nullptr;
+  if (n <= 1 || n > INT_MAX) return ADS_OK;
+  size_t sort_bytes = 0;
+  ADS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                           (uint32_t*)nullptr, (uint32_t*)nullptr, (int)n, 0, 8, st));
+  const size_t b4 = ((size_t)n * 4 + 255) / 256 * 256;
+  ADS_TRY(buf->alloc(4 * b4 + sort_bytes));
+  uint32_t* key = reinterpret_cast<uint32_t*>(buf->p);
+  uint32_t* key_out = reinterpret_cast<uint32_t*>(buf->p + b4);
+  uint32_t* idx = reinterpret_cast<uint32_t*>(buf->p + 2 * b4);
+  uint32_t* perm = reinterpret_cast<uint32_t*>(buf->p + 3 * b4);
+  work_key_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(
+      n, c_pidx, l->n_prec, l->pidx_p, l->fstart_p, l->fstop_p, key, idx);
+  ADS_LAUNCH_CHECK();
+  ADS_CUDA(cub::DeviceRadixSort::SortPairs(buf->p + 4 * b4, sort_bytes, key, key_out, idx, perm,
+                                           (int)n, 0, 8, st));
+  *order = perm;
+  return ADS_OK;
+}
+
 __global__ void idf_count_kernel(int64_t n, const float* mzl, GridView g, uint32_t* counts) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
@@ -498,7 +552,8 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
                 M6 = V + 15 * Fm, TMP = V + 16 * Fm, NZ = V + 17 * Fm, MED = V + 18 * Fm,
                 MEDF = MED + Cm, KEEP = MEDF + Cm;
 
-  for (int64_t q = t; q < a.n; q += a.T) {
+  for (int64_t qq = t; qq < a.n; qq += a.T) {
+    const int64_t q = a.order ? (int64_t)a.order[qq] : qq;
     a.o_found[q] = 0;
     const uint64_t x = a.c_pidx[q];
     const uint64_t cs64 = a.c_start[q], ce64 = a.c_stop[q], center = a.c_center[q];
@@ -748,7 +803,8 @@ __global__ void __launch_bounds__(kScoreBlock) quant_kernel(QuantArgs qa) {
   const int64_t FMZ = V, FRAW = V + Fm, NZ = V + 2 * Fm, TMP = V + 3 * Fm, MEDF = V + 18 * Fm,
                 KEEP = MEDF + 2 * Cm;
 
-  for (int64_t q = t; q < a.n; q += a.T) {
+  for (int64_t qq = t; qq < a.n; qq += a.T) {
+    const int64_t q = a.order ? (int64_t)a.order[qq] : qq;
     qa.o_nq[q] = 0;
     const uint64_t cs64 = a.c_start[q], ce64 = a.c_stop[q], center = a.c_center[q];
     if (ce64 <= cs64 || center < cs64 || center >= ce64) continue;
@@ -1053,6 +1109,8 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
     a.Fraw = Fraw;
     a.Cm = Cm;
     a.scratch = scratch.p;
+    DevBuf<char> order_buf;  // candidates grouped by work (kept until the kernel is done)
+    ADS_TRY(work_order(n, pidx, l, st, &order_buf, &a.order));
     a.T = T;
     a.o_pidx = f->pidx_p;
     a.o_rank = f->rank_p;
@@ -1186,6 +1244,8 @@ int quant_device(const AdsQuantParams* p, const AdsDia* d, AdsLib* l, int64_t n,
     a.Fraw = Fraw;
     a.Cm = Cm;
     a.scratch = scratch.p;
+    DevBuf<char> order_buf;  // candidates grouped by work (kept until the kernel is done)
+    ADS_TRY(work_order(n, pidx, l, st, &order_buf, &a.order));
     a.T = T;
     a.err = tmp.p + 1;
     qa.o_nq = r->nq_p;
