@@ -280,6 +280,7 @@ struct AdsLib {
   int device = 0;
   int64_t n_prec = 0, n_frag = 0;
   int64_t max_frag = 0;  // max fragments of one precursor
+  int64_t min_frag = 0;  // min fragments of one precursor
   ads::DevBuf<char> arena;  // every array below lives in this one allocation
   uint64_t* pidx_p = nullptr;  // precursor arrays, sorted by precursor_idx
   float* pmz_p = nullptr;

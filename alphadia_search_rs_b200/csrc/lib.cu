@@ -197,6 +197,7 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     if (!std::isfinite(prt[i]))
       return fail(ADS_ERR_INVALID_ARGUMENT, "precursor " + std::to_string(i) + ": RT is not finite");
     lib->max_frag = std::max<int64_t>(lib->max_frag, (int64_t)(fe[i] - fs[i]));
+    lib->min_frag = i == 0 ? (int64_t)(fe[i] - fs[i]) : std::min<int64_t>(lib->min_frag, (int64_t)(fe[i] - fs[i]));
   }
   if (a->precursor_rt_tolerance) {
     ADS_TRY(host_view(a->precursor_rt_tolerance, P, L, tol_store, &tol));

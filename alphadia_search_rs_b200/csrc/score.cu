@@ -381,7 +381,8 @@ __global__ void work_key_kernel(int64_t n, const uint64_t* c_pidx, int64_t P, co
 int work_order(int64_t n, const uint64_t* c_pidx, const AdsLib* l, cudaStream_t st, DevBuf<char>* buf,
                const uint32_t** order) {
   *order = nullptr;
-  if (n <= 1 || n > INT_MAX) return ADS_OK;
+  // nothing to group when every precursor has the same number of library fragments
+  if (n <= 1 || n > INT_MAX || l->min_frag == l->max_frag) return ADS_OK;
   size_t sort_bytes = 0;
   ADS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
                                            (uint32_t*)nullptr, (uint32_t*)nullptr, (int)n, 0, 8, st));
@@ -539,6 +540,9 @@ __device__ __forceinline__ void normalize_rows(const Scr& s, int64_t XIC, int64_
   }
 }
 
+// ORDERED: threads take the candidates in a.order (else in index order; compiled
+// apart because the indirection changes the code of the whole loop).
+template <bool ORDERED>
 __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= a.T) return;
@@ -553,7 +557,7 @@ __global__ void __launch_bounds__(kScoreBlock) score_kernel(ScoreArgs a) {
                 MEDF = MED + Cm, KEEP = MEDF + Cm;
 
   for (int64_t qq = t; qq < a.n; qq += a.T) {
-    const int64_t q = a.order ? (int64_t)a.order[qq] : qq;
+    const int64_t q = ORDERED ? (int64_t)a.order[qq] : qq;
     a.o_found[q] = 0;
     const uint64_t x = a.c_pidx[q];
     const uint64_t cs64 = a.c_start[q], ce64 = a.c_stop[q], center = a.c_center[q];
@@ -792,6 +796,7 @@ __global__ void quant_span_kernel(int64_t n, const uint64_t* center, const uint6
   }
 }
 
+template <bool ORDERED>
 __global__ void __launch_bounds__(kScoreBlock) quant_kernel(QuantArgs qa) {
   const ScoreArgs& a = qa.s;
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -804,7 +809,7 @@ __global__ void __launch_bounds__(kScoreBlock) quant_kernel(QuantArgs qa) {
                 KEEP = MEDF + 2 * Cm;
 
   for (int64_t qq = t; qq < a.n; qq += a.T) {
-    const int64_t q = a.order ? (int64_t)a.order[qq] : qq;
+    const int64_t q = ORDERED ? (int64_t)a.order[qq] : qq;
     qa.o_nq[q] = 0;
     const uint64_t cs64 = a.c_start[q], ce64 = a.c_stop[q], center = a.c_center[q];
     if (ce64 <= cs64 || center < cs64 || center >= ce64) continue;
@@ -1120,7 +1125,10 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
     ADS_CUDA(cudaEventCreate(&ev.a));
     ADS_CUDA(cudaEventCreate(&ev.b));
     ADS_CUDA(cudaEventRecord(ev.a, st));
-    score_kernel<<<(int)((T + kScoreBlock - 1) / kScoreBlock), kScoreBlock, 0, st>>>(a);
+    if (a.order)
+      score_kernel<true><<<(int)((T + kScoreBlock - 1) / kScoreBlock), kScoreBlock, 0, st>>>(a);
+    else
+      score_kernel<false><<<(int)((T + kScoreBlock - 1) / kScoreBlock), kScoreBlock, 0, st>>>(a);
     ADS_LAUNCH_CHECK();
     ADS_CUDA(cudaEventRecord(ev.b, st));
     f->found.resize((size_t)n);
@@ -1267,7 +1275,10 @@ int quant_device(const AdsQuantParams* p, const AdsDia* d, AdsLib* l, int64_t n,
     ADS_CUDA(cudaEventCreate(&ev.a));
     ADS_CUDA(cudaEventCreate(&ev.b));
     ADS_CUDA(cudaEventRecord(ev.a, st));
-    quant_kernel<<<(int)((T + kScoreBlock - 1) / kScoreBlock), kScoreBlock, 0, st>>>(qa);
+    if (qa.s.order)
+      quant_kernel<true><<<(int)((T + kScoreBlock - 1) / kScoreBlock), kScoreBlock, 0, st>>>(qa);
+    else
+      quant_kernel<false><<<(int)((T + kScoreBlock - 1) / kScoreBlock), kScoreBlock, 0, st>>>(qa);
     ADS_LAUNCH_CHECK();
     ADS_CUDA(cudaEventRecord(ev.b, st));
     // where each candidate's rows go: exclusive scans of the kept-fragment counts
