@@ -427,32 +427,43 @@ int plan_classes(int64_t c_max, int fixed_S, LenClasses* out) {
   return n + 1;
 }
 
-template <int H, bool FAST>
+template <int H, bool FAST, bool STATS>
 void (*pick_for_h(int S, bool grow))(SearchArgs) {
-  if (grow) return search_kernel<H, kGrowLaneCycles, FAST, true>;
+  if (grow) return search_kernel<H, kGrowLaneCycles, FAST, true, STATS>;
   switch (S) {
-    case 4: return search_kernel<H, 4, FAST, false>;
-    case 8: return search_kernel<H, 8, FAST, false>;
-    case 10: return search_kernel<H, 10, FAST, false>;
-    case 12: return search_kernel<H, 12, FAST, false>;
-    default: return search_kernel<H, 16, FAST, false>;
+    case 4: return search_kernel<H, 4, FAST, false, STATS>;
+    case 8: return search_kernel<H, 8, FAST, false, STATS>;
+    case 10: return search_kernel<H, 10, FAST, false, STATS>;
+    case 12: return search_kernel<H, 12, FAST, false, STATS>;
+    default: return search_kernel<H, 16, FAST, false, STATS>;
   }
 }
 
+// The statistics pass counts gather work, which the half width does not change: it
+// runs the generic-h instances with the counters compiled in.
 template <bool FAST>
-void (*pick_for_precision(int h, int S, bool grow))(SearchArgs) {
+void (*pick_for_precision(int h, int S, bool grow, bool stats))(SearchArgs) {
+  if (stats) return pick_for_h<0, FAST, true>(S, grow);
   switch (h) {
-    case 10: return pick_for_h<10, FAST>(S, grow);
-    case 11: return pick_for_h<11, FAST>(S, grow);
-    case 16: return pick_for_h<16, FAST>(S, grow);
-    default: return pick_for_h<0, FAST>(S, grow);
+    case 10: return pick_for_h<10, FAST, false>(S, grow);
+    case 11: return pick_for_h<11, FAST, false>(S, grow);
+    case 16: return pick_for_h<16, FAST, false>(S, grow);
+    default: return pick_for_h<0, FAST, false>(S, grow);
   }
 }
 
 // fast: BF16 intensity storage with the fast f32 arithmetic (ADS_PRECISION_BF16);
-// grow: working sets in global memory (long windows; S must be kGrowLaneCycles)
-void (*pick_search_kernel(int h, int S, bool fast, bool grow))(SearchArgs) {
-  return fast ? pick_for_precision<true>(h, S, grow) : pick_for_precision<false>(h, S, grow);
+// grow: working sets in global memory (long windows; S must be kGrowLaneCycles);
+// stats: the statistics pass's instances (work counters compiled in)
+void (*pick_search_kernel(int h, int S, bool fast, bool grow, bool stats))(SearchArgs) {
+  return fast ? pick_for_precision<true>(h, S, grow, stats)
+              : pick_for_precision<false>(h, S, grow, stats);
+}
+
+// Largest block (in warps) an instance may launch: its launch bounds (LaunchShape); the
+// statistics pass runs the generic-h instances (256 threads).
+int max_warps_per_block(bool fast, int h, bool grow, bool stats) {
+  return (stats ? 256 : launch_threads(h, fast, grow)) / 32;
 }
 
 // Long-window launches: blocks whose working sets fit kGrowBudgetBytes (at least one).
@@ -916,18 +927,18 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     // which packs long-window classes into shared memory better than 8
     bool grow = cmax_b > kSmemMaxCycles;
     int nw = s->o.warps_per_block > 0 ? s->o.warps_per_block : kDefaultWarpsPerBlock;
-    nw = std::max(1, std::min(nw, 8));
     if (!grow && search_smem_bytes(1, S, s->h, (cmax_b + 32 * S - 1) / (32 * S) * 32 * S, false) >
                      (size_t)max_smem)
       grow = true;  // a very wide kernel: even one warp's plan exceeds shared memory
     if (grow) S = kGrowLaneCycles;
+    nw = std::max(1, std::min(nw, max_warps_per_block(bf16, s->h, grow, s->stats_on)));
     const int ncell_b = (cmax_b + 32 * S - 1) / (32 * S) * 32 * S;
     while (nw > 1 && search_smem_bytes(nw, S, s->h, ncell_b, grow) > (size_t)max_smem) --nw;
     const size_t smem = search_smem_bytes(nw, S, s->h, ncell_b, grow);
     if (smem > (size_t)max_smem)
       return fail(ADS_ERR_INTERNAL, "search kernel plan exceeds shared memory (" +
                                         std::to_string(cmax_b) + " cycles)");
-    void (*kern)(SearchArgs) = pick_search_kernel(s->h, S, bf16, grow);
+    void (*kern)(SearchArgs) = pick_search_kernel(s->h, S, bf16, grow, s->stats_on);
     ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
     ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
@@ -1030,6 +1041,8 @@ int autotune(AdsSelection* s, const AdsDia* d, const AdsLib* l, int32_t repeats,
     scratch.device = s->device;
     int rc = ADS_OK;
     for (int nw : {2, 4, 8}) {
+      if (nw > max_warps_per_block(s->o.precision == ADS_PRECISION_BF16, s->h, false, false))
+        continue;
       for (int S : {0, 4, 8, 10, 12, 16}) {
         if (S != 0 && (int64_t)32 * S * 8 < key.c_max) continue;  // more than 8 passes
         s->o.warps_per_block = nw;
@@ -1594,7 +1607,7 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   if (smem > (size_t)max_smem)
     return fail(ADS_ERR_INTERNAL, "search kernel plan exceeds shared memory (" +
                                       std::to_string(c_max) + " cycles)");
-  void (*kern)(SearchArgs) = pick_search_kernel(h, S, false, grow);
+  void (*kern)(SearchArgs) = pick_search_kernel(h, S, false, grow, false);
   ADS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));

@@ -150,10 +150,45 @@ __host__ __device__ inline size_t search_smem_bytes(int nw, int S, int h, int nc
   return (size_t)(block_header_words(h) + (grow ? 0 : nw * warp_plan(S, h, ncell).total)) * 4;
 }
 
-// Per-warp work counters (the statistics pass); 32 bits suffice for one warp's
-// share of a launch.
+// Launch bounds of an instance.  The FP32 shared-memory instances for half widths 10
+// and 11 (kernel sizes 20-22) at 128 threads and 5 blocks per SM: up to 102 registers,
+// 20 warps (on 3000 x 300 data with 301-cycle windows 9 % faster than 256 x 2, without
+// spills worth noting).  Everything else at 256 x 2 (128 registers): the BF16 instances
+// (the 20-warp shape was 1.5 % slower on the uneven workload), half width 16 (spilled
+// up to 256 bytes and ran 13 % slower at kernel size 31), the generic half width and the
+// global-memory (long-window) instances.
+template <int H, bool FAST, bool GROW>
+struct LaunchShape {
+  static constexpr bool narrow = !FAST && !GROW && (H == 10 || H == 11);
+  static constexpr int threads = narrow ? 128 : 256;
+  static constexpr int blocks = narrow ? 5 : 2;
+};
+__host__ __device__ constexpr int launch_threads(int h, bool fast, bool grow) {
+  return (!fast && !grow && (h == 10 || h == 11)) ? 128 : 256;
+}
+
+// Per-warp work counters of the statistics pass (ON); 32 bits suffice for one warp's
+// share of a launch.  In the searching instances (ON = false) they hold nothing and
+// compile to no instruction.
+template <bool ON>
+struct Count;
+template <>
+struct Count<true> {
+  unsigned int v = 0;
+  __device__ Count& operator+=(unsigned int x) {
+    v += x;
+    return *this;
+  }
+  __device__ unsigned int get() const { return v; }
+};
+template <>
+struct Count<false> {
+  __device__ Count& operator+=(unsigned int) { return *this; }
+  __device__ unsigned int get() const { return 0u; }
+};
+template <bool ON>
 struct Counters {
-  unsigned int read = 0, acc = 0, off = 0, pairs = 0, bins1 = 0, frag = 0;
+  Count<ON> read, acc, off, pairs, bins1, frag;
 };
 
 // The rare case of add_chunk: lanes that hit the same cycle are grouped and summed
@@ -185,12 +220,13 @@ static __device__ __noinline__ void add_chunk_grouped(bool inc, int cell, int ad
 // reads back another number shares the cycle, and only then are the lanes grouped
 // and summed by their lowest lane one rounded add at a time.
 // Accepted cells are also appended to `touched` (the next row clears them).
+template <class Acc>
 __device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v, int lane,
                                           float* row, uint32_t* bm, uint32_t* tags, float* scr,
-                                          unsigned int& n_acc, uint16_t* touched, int& n_touched) {
+                                          Acc& n_acc, uint16_t* touched, int& n_touched) {
   const unsigned act = __ballot_sync(kFull, inc);
   if (act == 0) return;
-  n_acc += __popc(act);
+  n_acc += (unsigned int)__popc(act);
   if (inc) {
     const int at = n_touched + __popc(act & ((1u << lane) - 1u));
     if (at < kTouchCap) touched[at] = (uint16_t)cell;
@@ -275,19 +311,20 @@ __device__ __forceinline__ bool scans(const SearchArgs& a, uint32_t n) {
 }
 
 // `pre`: the range's first batch, already loaded (or null).
-template <int S, bool FAST>
+template <int S, bool FAST, bool STATS>
 __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64_t wbase,
                                             uint32_t b0, uint32_t b1, uint32_t rs, uint32_t re,
                                             int cs, int ce, int lane, float* row, int off,
                                             uint32_t* bm, uint32_t* tags, float* scr,
-                                            Counters& k, const ScanBatch<kPrefetchChunks<FAST>>* pre,
+                                            Counters<STATS>& k,
+                                            const ScanBatch<kPrefetchChunks<FAST>>* pre,
                                             uint16_t* touched,
                                             int& n_touched) {
   if (re <= rs) return;
   const uint32_t n = re - rs;
   const WinEntries e = win_entries(a, wbase);
   if (scans(a, n)) {
-    k.read += n;
+    k.read += (unsigned int)n;
     constexpr int NC = kPrefetchChunks<FAST>;
     for (uint32_t q0 = rs; q0 < re; q0 += 32 * NC) {
       ScanBatch<NC> bt;
@@ -336,7 +373,7 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
         const int64_t end = pos + lower_bound_u16(cy + pos, s1 - pos, ce);
         cnt = end - pos;
       }
-      k.off += 2 * __popc(__ballot_sync(kFull, vb));
+      k.off += 2u * (unsigned int)__popc(__ballot_sync(kFull, vb));
       int64_t incl = cnt;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -345,7 +382,7 @@ __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64
       }
       const int64_t total = __shfl_sync(kFull, incl, 31);
       const int64_t excl = incl - cnt;
-      k.read += total;
+      k.read += (unsigned int)total;
       for (int64_t t0 = 0; t0 < total; t0 += 32) {
         const int64_t t = t0 + lane;
         int l = 0;
@@ -515,11 +552,12 @@ struct PairCursor {
 // Gathers fragment f's XIC row: its (fragment, window) pairs in window order (the
 // reference's DenseXICObservation::new, src/dense_xic_observation/mod.rs:30-64),
 // then prefetches the first batch of the next fragment's first pair.
-template <int S, bool FAST>
+template <int S, bool FAST, bool STATS>
 __device__ __forceinline__ void gather_row(const SearchArgs& a, int64_t p, int f, int nwin,
                                            int npairs, int cs, int ce, int lane,
                                            PairCursor<FAST>& pc, float* row, int off,
-                                           uint32_t* bm, uint32_t* tags, float* scr, Counters& k,
+                                           uint32_t* bm, uint32_t* tags, float* scr,
+                                           Counters<STATS>& k,
                                            uint16_t* touched, int& n_touched) {
   for (int wi = 0; wi < nwin; ++wi) {
     const int pi = f * nwin + wi;
@@ -552,10 +590,10 @@ __device__ __forceinline__ void gather_row(const SearchArgs& a, int64_t p, int f
     const int qw = __shfl_sync(kFull, pc.wsel, q);
     const int64_t qbase = __shfl_sync(kFull, pc.wbase, q);
     if (qb1 <= qb0) continue;
-    k.off += 2;
-    k.pairs += 1;
+    k.off += 2u;
+    k.pairs += 1u;
     k.bins1 += qb1 - qb0 + 1;
-    gather_pair<S, FAST>(a, qw, qbase, qb0, qb1, qrs, qre, cs, ce, lane, row, off, bm, tags, scr,
+    gather_pair<S, FAST, STATS>(a, qw, qbase, qb0, qb1, qrs, qre, cs, ce, lane, row, off, bm, tags, scr,
                          k, pi == pc.pre_pi ? &pc.pre : nullptr, touched, n_touched);
   }
   __syncwarp();
@@ -688,22 +726,26 @@ __device__ __forceinline__ void pick_top_k(const SearchArgs& a, int64_t p, int c
 }
 
 // Per-warp work counters to the statistics pass's totals.
-__device__ __forceinline__ void flush_counters(const SearchArgs& a, const Counters& k, int lane) {
-  if (a.stats && lane == 0) {
-    atomicAdd(a.stats + 0, (unsigned long long)k.pairs);
-    atomicAdd(a.stats + 1, (unsigned long long)k.bins1);
-    atomicAdd(a.stats + 2, (unsigned long long)k.frag);
-    atomicAdd(a.stats + 3, (unsigned long long)k.read);
-    atomicAdd(a.stats + 4, (unsigned long long)k.acc);
-    atomicAdd(a.stats + 5, (unsigned long long)k.off);
+template <bool STATS>
+__device__ __forceinline__ void flush_counters(const SearchArgs& a, const Counters<STATS>& k,
+                                               int lane) {
+  if (STATS && a.stats && lane == 0) {
+    atomicAdd(a.stats + 0, (unsigned long long)k.pairs.get());
+    atomicAdd(a.stats + 1, (unsigned long long)k.bins1.get());
+    atomicAdd(a.stats + 2, (unsigned long long)k.frag.get());
+    atomicAdd(a.stats + 3, (unsigned long long)k.read.get());
+    atomicAdd(a.stats + 4, (unsigned long long)k.acc.get());
+    atomicAdd(a.stats + 5, (unsigned long long)k.off.get());
   }
 }
 
 // GROW: the warp's working set (row, tags, bitmap, scores, lists, maxima) lives in
 // a global buffer of P.total words per warp (`a.grow`) instead of shared memory, for
 // RT windows longer than kSmemMaxCycles; the code and every operation are the same.
-template <int H, int S, bool FAST, bool GROW>
-__global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
+// STATS: the statistics pass's work counters (compiled in only for it).
+template <int H, int S, bool FAST, bool GROW, bool STATS>
+__global__ void __launch_bounds__(LaunchShape<H, FAST, GROW>::threads, LaunchShape<H, FAST, GROW>::blocks)
+    search_kernel(SearchArgs a) {
   extern __shared__ __align__(16) float smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int h = H > 0 ? H : a.h;
@@ -730,7 +772,7 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
   for (int i = threadIdx.x; i < kLnTableSize; i += blockDim.x) lnt[i] = a.ln_tab[i];
   for (int i = threadIdx.x; i <= a.h; i += blockDim.x) kw_s[i] = a.kw_dev ? a.kw_dev[i] : a.kw[i];
   __syncthreads();
-  Counters k;
+  Counters<STATS> k;
 
   const unsigned long long n_work = a.list ? (unsigned long long)*a.list_len
                                             : (unsigned long long)a.n_prec;
@@ -779,9 +821,8 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
       n_touched = 0;
       __syncwarp();
       // ---- 1. gather: the fragment's pairs in window order
-      const unsigned int acc0 = k.acc;
-      gather_row<S, FAST>(a, p, f, nwin, npairs, cs, ce, lane, pc, row, P.off, bm, tags, scr, k,
-                          touched, n_touched);
+      gather_row<S, FAST, STATS>(a, p, f, nwin, npairs, cs, ce, lane, pc, row, P.off, bm, tags,
+                                 scr, k, touched, n_touched);
       float wf = __shfl_sync(kFull, wf_lane, f & 31);
       if (f >= 32) wf = __ldg(a.fw + p * a.kf + f);
       if (!isfinite(wf)) {
@@ -794,7 +835,7 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
         __syncwarp();
         continue;
       }
-      if (k.acc == acc0) continue;  // empty row: every term is +0
+      if (n_touched == 0) continue;  // no entry accepted: every term is +0
       // ---- 2./3. convolution of this lane's cycles, then the score terms of its
       // non-zero outputs.  A zero output adds ln(1) * w = +0, which leaves a score as
       // it is, so only non-zero outputs of the valid range [h, C - h) are listed
@@ -884,5 +925,5 @@ __global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a) {
 
     pick_top_k<S>(a, p, cs, C, score, mval, midx, P.mx, lane);
   }
-  flush_counters(a, k, lane);
+  flush_counters<STATS>(a, k, lane);
 }

@@ -177,7 +177,8 @@ typedef struct {
   int32_t verbose;     /* 1: print the reference's two lines after each search
                           (src/peak_group_selection/mod.rs:123-125) */
   int32_t use_graph;   /* 1: capture the search pipeline in a CUDA graph and replay it */
-  int32_t warps_per_block; /* 0 = default (4); else 1..8 warps, one precursor each */
+  int32_t warps_per_block; /* 0 = default (4); else 1..8 warps, one precursor each
+                              (FP32 searches: at most 4) */
   int32_t blocks_per_sm;   /* 0 = autotuned/default */
   int32_t gather_mode;     /* 0 = automatic, 1 = always scan bin ranges, 2 = always
                               binary-search each bin (both are exact; for testing) */
@@ -271,7 +272,8 @@ int ads_selection_last_stats(AdsSelection* sel, int64_t* out, int64_t cap);
 int ads_selection_stage_times(AdsSelection* sel, float* ms, int64_t cap);
 /* Autotuner (an engine addition; the reference has no launch shapes to tune).
  * Times the search of `dia` x `lib` (`repeats` timed searches per shape, after
- * one warm-up) for warps per block 2, 4, 8 (precursors in flight per CTA) and cycles
+ * one warm-up) for warps per block 2, 4, 8 (precursors in flight per CTA; 2 and 4 for
+ * FP32) and cycles
  * per lane 0 (length classes), 4, 8, 10, 12, 16 (cycles per tile = 32 x that),
  * keeps the fastest in the selection's options and caches it per workload shape
  * (device, precision, kernel half width, longest RT window, precursors, fragments)
