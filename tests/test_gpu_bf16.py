@@ -132,3 +132,20 @@ def test_bf16_only_run_storage():
         PeakGroupScoring(ScoringParameters(), verbose=False).score(dia16, slib, cand)
     with pytest.raises(ValueError, match="bfloat16"):
         PeakGroupQuantification(QuantificationParameters(), verbose=False).quantify(dia16, slib, cand)
+
+
+@pytest.mark.parametrize("kernel_size,fwhm_rt", [(64, 12.0), (128, 30.0)])
+def test_bf16_wide_kernels_against_fp64_oracle(kernel_size, fwhm_rt):
+    """BF16 storage with Gaussian kernels wider than 62 (taps from device memory)."""
+    cfg, lib, run = synth.make_workload("tiny_long", "numpy")
+    la = synth.library_arrays(lib)
+    params = dict(cfg.params_dict(), kernel_size=kernel_size, fwhm_rt=fwhm_rt)
+    got, *_ = product_search(run, la, params, precision="bf16")
+    od, ol, tol = oracle_inputs(run, la)
+    ref = oracle.search(od, ol, oracle.Params(**params), rt_tolerance_per_precursor=tol,
+                        log_mode=oracle.LOG_RN, precision=1)
+    assert len(ref["rank"]) > 0
+    agree, errs = compare_to_fp64(got, ref)
+    assert agree >= 0.99, f"kernel_size {kernel_size}: top-k cycle agreement {agree:.4f}"
+    assert errs.max() <= SCORE_MAX_BF16
+    assert float(np.quantile(errs, 0.99)) <= SCORE_P99_BF16

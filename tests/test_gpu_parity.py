@@ -292,3 +292,23 @@ def test_wide_kernels(kernel_size, fwhm_rt):
     ref = oracle_search(run, la, params, oracle.LOG_RN)
     assert len(ref["rank"]) > 0
     assert_candidates_equal(got, ref, exact_scores=True, where=f"kernel_size {kernel_size}")
+
+
+def test_statistics_pass_with_wide_kernel_and_long_windows():
+    """The statistics pass runs the generic-half-width instances with the counters
+    compiled in: same candidates as the search, and counts that add up."""
+    from alphadia_search_rs_b200 import PeakGroupSelection
+
+    from _util import COLS, params_from
+
+    cfg, lib, run = synth.make_workload("tiny_long", "numpy")
+    la = synth.library_arrays(lib)
+    params = dict(cfg.params_dict(), kernel_size=101, fwhm_rt=25.0)
+    ref, dia, slib, _ = product_search(run, la, params)
+    sel = PeakGroupSelection(params_from(params), verbose=False)
+    sel.enable_stats(True)
+    got = dict(zip(COLS, sel.search(dia, slib).to_arrays()))
+    assert_candidates_equal(got, ref, exact_scores=True, where="statistics pass")
+    st = sel.last_stats()
+    assert st["pairs"] > 0 and st["entries_accumulated"] <= st["entries_read"]
+    assert st["fragments"] <= st["xic_cells"]
