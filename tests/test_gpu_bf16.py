@@ -5,7 +5,7 @@ Relative score error is taken against max(|s64|, 1e-3 * max |s64| of the
 precursor), because scores near zero are common at the RT-window edges.  Bounds:
   * top-k candidate cycles: at least 99.5% identical to the oracle's (99% on the
     few-hundred-precursor cases);
-  * scores: the north star's bound, 1e-3 relative, holds for the 99th percentile
+  * scores: the target bound, 1e-3 relative, holds for the 99th percentile
     and the median, and is asserted there.  It cannot hold for the maximum:
     bfloat16 keeps 8 significant bits, so a stored intensity may be off by up to
     u = 2^-8 = 3.9e-3 relative (just above a power of two), and a score column fed
