@@ -284,7 +284,8 @@ __global__ void cells_kernel(int64_t n, const int* nf, const int* cs, const int*
 }
 
 // 8 blocks of 256 threads per SM (32 registers): the kernel waits on its global loads,
-// so occupancy pays (0.33 -> 0.27 ms per cfg1 search against 4 blocks at 62 registers)
+// so occupancy pays (0.33 -> 0.27 ms per search of 200,000 precursors on 3000 x 300 data,
+// against 4 blocks at 62 registers)
 __global__ void __launch_bounds__(kPrepThreads, 8) prep_kernel(PrepArgs a) {
   extern __shared__ __align__(16) unsigned char prep_smem[];
   const int lane = threadIdx.x & 31;
