@@ -22,6 +22,7 @@
 #include <map>
 #include <tuple>
 #include <memory>
+#include <thread>
 
 #include <cuda_bf16.h>
 
@@ -1375,8 +1376,18 @@ int ads_candidates_copy_out(AdsCandidates* c, uint64_t* pidx, uint64_t* rank, fl
       if (col.dst)
         ADS_CUDA(cudaMemcpyAsync(col.dst, col.src, n * col.bytes, cudaMemcpyDeviceToHost,
                                  cudaStreamPerThread));
-    for (uint64_t* z : {scan_center, scan_start, scan_stop})
-      if (z) std::memset(z, 0, n * 8);
+    // the reference's scan_* columns are zero: written on the host while the copies
+    // run, one thread per column when they are large (one thread fills about 10 GB/s)
+    uint64_t* zeros[3] = {scan_center, scan_start, scan_stop};
+    if (n >= ((size_t)1 << 20)) {
+      std::vector<std::thread> fill;
+      for (uint64_t* z : zeros)
+        if (z) fill.emplace_back([z, n] { std::memset(z, 0, n * 8); });
+      for (auto& t : fill) t.join();
+    } else {
+      for (uint64_t* z : zeros)
+        if (z) std::memset(z, 0, n * 8);
+    }
     ADS_CUDA(cudaStreamSynchronize(cudaStreamPerThread));
     return ADS_OK;
   });
