@@ -180,9 +180,14 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
   else if (P)
     ADS_CUDA(cudaMemsetAsync(sort ? naa_in : lib->naa_p, 0, (size_t)P, st));
   ADS_TRY(copy_in(lib->fmz_p, a->fragment_mz, NF, L, st));
-  // fragment_mz_library defaults to fragment_mz (the IDF of scoring reads it)
-  ADS_TRY(copy_in(lib->fmzl_p, a->fragment_mz_library ? a->fragment_mz_library : a->fragment_mz, NF,
-                  L, st));
+  // fragment_mz_library (the IDF of scoring reads it) defaults to fragment_mz; when it
+  // is fragment_mz's own array it is copied on the device instead of uploaded again
+  if (!a->fragment_mz_library || a->fragment_mz_library == a->fragment_mz) {
+    if (NF) ADS_CUDA(cudaMemcpyAsync(lib->fmzl_p, lib->fmz_p, (size_t)NF * sizeof(float),
+                                     cudaMemcpyDeviceToDevice, st));
+  } else {
+    ADS_TRY(copy_in(lib->fmzl_p, a->fragment_mz_library, NF, L, st));
+  }
   ADS_TRY(copy_in(lib->fint_p, a->fragment_intensity, NF, L, st));
   ADS_TRY(copy_in(lib->fnum_p, a->fragment_number, NF, L, st));
   ADS_TRY(copy_in(lib->ftype_p, a->fragment_type, NF, L, st));

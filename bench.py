@@ -200,6 +200,14 @@ def library_tensors(lib: dict, device: str):
     return out
 
 
+def host_copies(tensors: dict, copy) -> dict:
+    """copy(t) of every tensor, one copy per distinct tensor: columns that are the same
+    array (the synthetic library's m/z and library m/z, RT and library RT) stay one
+    array on the host, as a caller's would."""
+    done = {}
+    return {k: done.setdefault(id(v), copy(v)) for k, v in tensors.items()}
+
+
 def sample_windows(cfg, requested: int) -> int:
     """MS2 windows of the CPU sample: as requested, else about 72 M peaks' worth
     (24 windows at 3000 cycles x 1000 peaks)."""
@@ -671,11 +679,14 @@ def e2e_search(ads, params, precision, dia, lib_np, n_cand, steps, local_rank, d
     out_t = [torch.empty(cap, dtype=torch.float32 if i == 2 else torch.uint64).pin_memory() for i in range(9)]
     out_np = tuple(t.numpy() for t in out_t)
     sel_e2e = ads.PeakGroupSelection(params, verbose=False, device=local_rank, precision=precision)
-    h2d = sum(lib_np[k].nbytes for k in ("precursor_idx", "precursor_mz", "precursor_rt",
-                                          "flat_frag_start_idx", "flat_frag_stop_idx", "fragment_mz",
-                                          "fragment_intensity", "fragment_number", "fragment_type"))
-    if "precursor_rt_tolerance" in lib_np:
-        h2d += lib_np["precursor_rt_tolerance"].nbytes
+    # what SpecLibFlat.from_arrays uploads (the arrays the reference's other columns
+    # name are kept on the host); fragment_mz_library only when it is its own array
+    copied = ["precursor_idx", "precursor_mz", "precursor_rt", "precursor_naa", "flat_frag_start_idx",
+              "flat_frag_stop_idx", "fragment_mz", "fragment_intensity", "fragment_number",
+              "fragment_type", "precursor_rt_tolerance"]
+    h2d = sum(lib_np[k].nbytes for k in copied if k in lib_np)
+    if lib_np["fragment_mz_library"].ctypes.data != lib_np["fragment_mz"].ctypes.data:
+        h2d += lib_np["fragment_mz_library"].nbytes
     times = []
     d2h = 0
     for i in range(steps + 1):
@@ -804,7 +815,7 @@ def run_ours(args, rank, world, local_rank):
     n_peaks_total = int(run["peak_mz"].numel())
     nf_raw = int(lib["fragment_mz"].numel())
     if not keep_inputs:  # the device copies inside DIAData/SpecLibFlat are all the search needs
-        lib_host_src = {k: v.cpu() for k, v in ltens.items()}
+        lib_host_src = host_copies(ltens, lambda v: v.cpu())
         del run, ltens
         ltens = lib_host_src
         torch.cuda.empty_cache()
@@ -815,7 +826,7 @@ def run_ours(args, rank, world, local_rank):
     head = timed[arms[0]]
     value = P * world * args.steps / (head["ms"] / 1e3)
 
-    lib_host = {k: v.cpu().pin_memory() for k, v in ltens.items()}
+    lib_host = host_copies(ltens, lambda v: v.cpu().pin_memory())
     lib_np = {k: v.numpy() for k, v in lib_host.items()}
     e2e = {prec: e2e_search(ads, params, prec, dia, lib_np, timed[prec]["n_cand"], args.e2e_steps,
                             local_rank, dist) for prec in arms}
