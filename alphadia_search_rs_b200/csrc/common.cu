@@ -99,6 +99,15 @@ void pool_free(int device, void* p) {
   cudaGetLastError();
 }
 
+void pool_free_async(int device, void* p, cudaStream_t st) {
+  DevicePool dp;
+  if (device_pool(device, &dp) != ADS_OK) return;
+  DeviceGuard dg(device);
+  cudaFreeAsync(p, st);
+  update_release_threshold(dp.pool);
+  cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- m/z grid
 
 // MZIndex::new / ppm_index (src/mz_index/mod.rs:8-25, 41-45): f32 geometric

@@ -74,6 +74,9 @@ struct DeviceGuard {
 constexpr uint64_t kPoolKeepBytes = uint64_t(4) << 30;
 int pool_alloc(int device, size_t bytes, void** out);
 void pool_free(int device, void* p);
+// Frees p once the work enqueued on `st` so far is done (no host synchronisation): for
+// memory that only `st` uses.
+void pool_free_async(int device, void* p, cudaStream_t st);
 
 // Owning device buffer (move-only) on the current device's pool.
 template <class T>
@@ -102,6 +105,12 @@ struct DevBuf {
   ~DevBuf() { release(); }
   void release() {
     if (p) pool_free(dev, p);
+    p = nullptr;
+    n = 0;
+  }
+  // release() for a buffer that only `st` has used: ordered after its work on `st`.
+  void release_async(cudaStream_t st) {
+    if (p) pool_free_async(dev, p, st);
     p = nullptr;
     n = 0;
   }

@@ -229,6 +229,9 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     launch_gather(P, pos_out, naa_in, lib->naa_p, st);
     if (lib->has_tol) launch_gather(P, pos_out, ptol_in, lib->ptol_p, st);
     ADS_LAUNCH_CHECK();
+    // the sort's temporary area is freed behind its last use on this stream: a
+    // library built while searches run elsewhere on the device does not wait for them
+    tmp.release_async(st);
   } else if (P > 0) {
     iota_kernel<<<(int)std::min<int64_t>((P + 255) / 256, 4096), 256, 0, st>>>(P, lib->prow_p);
     ADS_LAUNCH_CHECK();
