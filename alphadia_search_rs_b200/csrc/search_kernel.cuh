@@ -122,8 +122,8 @@ __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
   int o = 0;
   w.row = o;
   o += w.row_words;
-  w.tags = o;
-  o += ncell;
+  w.tags = o;  // one byte per cell: the lane that wrote it last
+  o += (ncell + 3) / 4;
   w.lead = h > kBitOff ? (h - kBitOff + 31) / 32 : 0;
   w.bw = (ncell + h + kBitOff + 31) / 32 + 2;
   w.bm = o + w.lead;
@@ -138,10 +138,17 @@ __host__ __device__ inline WarpPlan warp_plan(int S, int h, int ncell) {
   w.lst = o;  // one pass of non-zero convolved values: (value, score address) pairs
   o += 2 * 32 * S;
   w.mx = maxima_cap(ncell);
-  w.mval = o;
-  o += w.mx;
-  w.midx = o;
-  o += w.mx;
+  if (2 * w.mx <= 2 * 32 * S) {
+    // the maxima are collected after the precursor's last row is scored, when the
+    // output list is free
+    w.mval = w.lst;
+    w.midx = w.lst + w.mx;
+  } else {
+    w.mval = o;
+    o += w.mx;
+    w.midx = o;
+    o += w.mx;
+  }
   w.total = (o + 3) & ~3;
   return w;
 }
@@ -222,7 +229,7 @@ static __device__ __noinline__ void add_chunk_grouped(bool inc, int cell, int ad
 // Accepted cells are also appended to `touched` (the next row clears them).
 template <class Acc>
 __device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v, int lane,
-                                          float* row, uint32_t* bm, uint32_t* tags, float* scr,
+                                          float* row, uint32_t* bm, uint8_t* tags, float* scr,
                                           Acc& n_acc, uint16_t* touched, int& n_touched) {
   const unsigned act = __ballot_sync(kFull, inc);
   if (act == 0) return;
@@ -232,9 +239,9 @@ __device__ __forceinline__ void add_chunk(bool inc, int cell, int addr, float v,
     if (at < kTouchCap) touched[at] = (uint16_t)cell;
   }
   n_touched += __popc(act);
-  if (inc) tags[cell] = (uint32_t)lane;
+  if (inc) tags[cell] = (uint8_t)lane;
   __syncwarp();
-  const bool dup = inc && tags[cell] != (uint32_t)lane;
+  const bool dup = inc && tags[cell] != (uint8_t)lane;
   const int bit = cell + kBitOff;
   if (!__any_sync(kFull, dup)) {
     if (inc) {
@@ -315,7 +322,7 @@ template <int S, bool FAST, bool STATS>
 __device__ __forceinline__ void gather_pair(const SearchArgs& a, int wsel, int64_t wbase,
                                             uint32_t b0, uint32_t b1, uint32_t rs, uint32_t re,
                                             int cs, int ce, int lane, float* row, int off,
-                                            uint32_t* bm, uint32_t* tags, float* scr,
+                                            uint32_t* bm, uint8_t* tags, float* scr,
                                             Counters<STATS>& k,
                                             const ScanBatch<kPrefetchChunks<FAST>>* pre,
                                             uint16_t* touched,
@@ -556,7 +563,7 @@ template <int S, bool FAST, bool STATS>
 __device__ __forceinline__ void gather_row(const SearchArgs& a, int64_t p, int f, int nwin,
                                            int npairs, int cs, int ce, int lane,
                                            PairCursor<FAST>& pc, float* row, int off,
-                                           uint32_t* bm, uint32_t* tags, float* scr,
+                                           uint32_t* bm, uint8_t* tags, float* scr,
                                            Counters<STATS>& k,
                                            uint16_t* touched, int& n_touched) {
   for (int wi = 0; wi < nwin; ++wi) {
@@ -755,7 +762,7 @@ __global__ void __launch_bounds__(LaunchShape<H, FAST, GROW>::threads, LaunchSha
   float* wb = GROW ? a.grow + ((size_t)blockIdx.x * (blockDim.x >> 5) + warp) * (size_t)P.total
                    : smem_raw + block_header_words(h) + warp * P.total;
   float* row = wb + P.row;
-  uint32_t* tags = reinterpret_cast<uint32_t*>(wb + P.tags);
+  uint8_t* tags = reinterpret_cast<uint8_t*>(wb + P.tags);
   uint32_t* bm = reinterpret_cast<uint32_t*>(wb + P.bm);
   float* scr = wb + P.scr;
   float* score = wb + P.score;

@@ -150,9 +150,11 @@ class ClockSampler:
         for _, r in self.samples:
             seen |= r
         reasons = sorted(n for bit, n in names.items() if seen & bit)
+        share = {n: round(sum(1 for _, r in self.samples if r & bit) / len(self.samples), 4)
+                 for bit, n in names.items() if seen & bit}
         med = statistics.median([s for s, _ in self.samples]) if self.samples else None
         return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": reasons,
-                "samples": len(self.samples)}
+                "reason_share": share, "samples": len(self.samples)}
 
 
 # --------------------------------------------------------------- workload
