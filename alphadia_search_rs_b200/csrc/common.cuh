@@ -306,12 +306,30 @@ struct AdsLib {
   uint8_t* ftype_p = nullptr;
   bool has_tol = false;
   float max_tol = 0.0f;
+  // recorded after the library's device-side preparation (the precursor sort); every
+  // stream that reads the arrays waits on it (lib_ready_on)
+  cudaEvent_t ready = nullptr;
   // InverseDocumentFrequency (src/idf/mod.rs:13-33): fragments of the library per
   // m/z grid bin, built on the first scoring call
   std::mutex mu;
   ads::DevBuf<uint32_t> idf_counts;
   float idf_total = -1.0f;  // fragments the histogram counts (< 0: this library's own)
+  AdsLib() = default;
+  AdsLib(const AdsLib&) = delete;
+  AdsLib& operator=(const AdsLib&) = delete;
+  ~AdsLib() {
+    if (ready) cudaEventDestroy(ready);
+  }
 };
+
+namespace ads {
+// Orders `st` after the library's preparation (from_arrays returns once its uploads
+// have landed; the sort behind them may still be queued).
+inline int lib_ready_on(const AdsLib* l, cudaStream_t st) {
+  if (l->ready) ADS_CUDA(cudaStreamWaitEvent(st, l->ready, 0));
+  return ADS_OK;
+}
+}  // namespace ads
 
 // Candidate columns on the device (CandidateCollection, src/candidate/entry.rs:41-179).
 struct AdsCandidates {

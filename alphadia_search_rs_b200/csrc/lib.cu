@@ -191,6 +191,14 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
   ADS_TRY(copy_in(lib->fint_p, a->fragment_intensity, NF, L, st));
   ADS_TRY(copy_in(lib->fnum_p, a->fragment_number, NF, L, st));
   ADS_TRY(copy_in(lib->ftype_p, a->fragment_type, NF, L, st));
+  // the caller's arrays may be released once the copies above have landed
+  cudaEvent_t copied = nullptr;
+  ADS_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+  struct EventGuard {
+    cudaEvent_t e;
+    ~EventGuard() { cudaEventDestroy(e); }
+  } eg{copied};
+  ADS_CUDA(cudaEventRecord(copied, st));
 
   // validation of the per-precursor arrays (the reference panics on these), on the
   // host while the copies above are in flight; on failure the buffers are released
@@ -236,7 +244,13 @@ int lib_create(const AdsLibArrays* a, int device, AdsLib** out) {
     iota_kernel<<<(int)std::min<int64_t>((P + 255) / 256, 4096), 256, 0, st>>>(P, lib->prow_p);
     ADS_LAUNCH_CHECK();
   }
-  ADS_CUDA(cudaStreamSynchronize(st));
+  // The sort and gathers need SMs, which a search already running elsewhere on the
+  // device may hold until it ends: waiting for them here would keep the caller from
+  // enqueueing its next search behind that one.  Readers of the library wait on
+  // `ready` instead; the host waits for the uploads only.
+  ADS_CUDA(cudaEventCreateWithFlags(&lib->ready, cudaEventDisableTiming));
+  ADS_CUDA(cudaEventRecord(lib->ready, st));
+  ADS_CUDA(cudaEventSynchronize(copied));
   *out = lib.release();
   return ADS_OK;
 }

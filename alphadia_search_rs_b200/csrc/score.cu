@@ -1021,6 +1021,7 @@ int quant_assemble(AdsQuant* r, const uint64_t* d_off, const int* d_pos, cudaStr
 int ensure_idf(AdsLib* l, const GridView& g, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(l->mu);
   if (l->idf_counts.p) return ADS_OK;
+  ADS_TRY(lib_ready_on(l, st));
   ADS_TRY(l->idf_counts.alloc(g.n));
   ADS_CUDA(cudaMemsetAsync(l->idf_counts.p, 0, (size_t)g.n * 4, st));
   if (l->n_frag > 0) {
@@ -1043,6 +1044,7 @@ int score_device(const AdsScoringParams* p, const AdsDia* d, AdsLib* l, int64_t 
     return fail(ADS_ERR_INVALID_ARGUMENT, "mass_tolerance is NaN");
   if (p->top_k_fragments < 0) return fail(ADS_ERR_INVALID_ARGUMENT, "top_k_fragments < 0");
   cudaStream_t st = cudaStreamPerThread;
+  ADS_TRY(lib_ready_on(l, st));
   GridView g;
   ADS_TRY(device_grid(d->device, &g));
   ADS_TRY(ensure_idf(l, g, st));
@@ -1163,6 +1165,7 @@ int quant_device(const AdsQuantParams* p, const AdsDia* d, AdsLib* l, int64_t n,
     return fail(ADS_ERR_INVALID_ARGUMENT, "tolerance_ppm is NaN");
   if (p->top_k_fragments < 0) return fail(ADS_ERR_INVALID_ARGUMENT, "top_k_fragments < 0");
   cudaStream_t st = cudaStreamPerThread;
+  ADS_TRY(lib_ready_on(l, st));
   GridView g;
   ADS_TRY(device_grid(d->device, &g));
   auto r = std::make_unique<AdsQuant>();

@@ -750,6 +750,7 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     return fail(ADS_ERR_INVALID_ARGUMENT, "handles live on different devices");
   DeviceGuard dg(s->device);
   cudaStream_t st = s->o.stream ? (cudaStream_t)s->o.stream : s->stream;
+  if (!capturing) ADS_TRY(lib_ready_on(l, st));  // (a captured search replays after this one)
   if (!c->done) {
     ADS_CUDA(cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming));
   } else if (!capturing) {
@@ -1494,6 +1495,11 @@ int select_noalloc(const AdsDia* d, const AdsLib* l, const AdsSelectionParams* p
   char* base = nullptr;
   ADS_TRY(noalloc_scratch(d->device, &base));
   const cudaStream_t st = (cudaStream_t)stream;
+  // after the library's preparation; a capturing stream cannot wait on work outside
+  // its capture, so there the library must be prepared already (documented)
+  cudaStreamCaptureStatus capst = cudaStreamCaptureStatusNone;
+  ADS_CUDA(cudaStreamIsCapturing(st, &capst));
+  if (capst == cudaStreamCaptureStatusNone) ADS_TRY(lib_ready_on(l, st));
 
   // the same launch shape as ads_select with default engine options
   const int64_t P = l->n_prec;

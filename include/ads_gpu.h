@@ -124,6 +124,11 @@ int ads_selftest_ln(int device, uint32_t lo_bits, uint32_t hi_bits, int64_t* mis
  * charge, loss type, position) may be NULL.  precursor_rt_tolerance is an
  * extension: an optional per-precursor RT half-window in seconds that replaces
  * SelectionParameters.rt_tolerance for that precursor (NULL = the global value).
+ * ads_lib_create returns once the arrays have been copied (the caller may release
+ * them); the sort on the device may still be queued behind other work, and every
+ * call that reads the library orders itself after it.  Inside a stream capture
+ * (ads_select_noalloc) the library must already be prepared: synchronise, or search
+ * it once outside the capture, first.
  */
 typedef struct AdsLib AdsLib;
 
