@@ -721,7 +721,8 @@ def e2e_stream(ads, params, precision, dia, lib_np, n_cand, steps, local_rank, d
     candidates back (DeviceCandidates.copy_out into pinned arrays) while step i's runs;
     two candidate collections alternate.  Every step's upload, search and read-back
     lies inside the timed region (wall clock from the first upload to the last
-    read-back, over the steps).  The libraries are released after the timed region."""
+    read-back, over the steps), which follows one untimed pass of the same length.  The
+    libraries are released after each pass."""
     import torch
 
     device = f"cuda:{local_rank}"
@@ -743,7 +744,10 @@ def e2e_stream(ads, params, precision, dia, lib_np, n_cand, steps, local_rank, d
                 d2h = n * (5 * 8 + 4)  # five u64 columns and the f32 score (scan_* are zero)
         return libs, d2h
 
-    warm, _ = run(2)  # sizes the selection's and the collections' buffers
+    # an untimed pass of the same length first: it sizes the selection's and the
+    # collections' buffers and grows the device memory pool to hold a pass's libraries
+    # (the first pass at cfg4 took up to 0.8 s in one allocation; later passes reuse)
+    warm, _ = run(steps)
     del warm
     torch.cuda.synchronize()
     t0 = time.perf_counter()
