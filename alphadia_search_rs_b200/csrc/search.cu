@@ -1085,12 +1085,22 @@ int autotune(AdsSelection* s, const AdsDia* d, const AdsLib* l, int32_t repeats,
 }
 
 // Everything a captured search depends on: the handles and every buffer address.
+// Everything a captured pipeline bakes in: the handles, every buffer it reads or
+// writes, and the run- and library-derived sizes its launch plan depends on (a handle
+// released and another created at the same address must not replay a stale graph).
 std::vector<const void*> graph_key(const AdsSelection* s, const AdsDia* d, const AdsLib* l,
                                    const AdsCandidates* c) {
+  auto v = [](int64_t x) { return reinterpret_cast<const void*>(static_cast<intptr_t>(x)); };
+  uint32_t tol_bits = 0;
+  std::memcpy(&tol_bits, &l->max_tol, sizeof(tol_bits));
   return {d, l, c, c->arena.p, s->nf.p, s->cs.p, s->ce.p, s->nwin.p, s->wins.p, s->fw.p,
           s->blo.p, s->bhi.p, s->keep.p, s->cand_n.p, s->cand_score.p, s->cand_center.p,
           s->work.p, s->class_lists.p, s->block_sums.p, s->stats_on ? s->stats.p : nullptr,
-          d->intens_bf16.p, s->grow.p};
+          d->intens_bf16.p, s->grow.p, s->taps.p,
+          d->slice_starts.p, d->cycles.p, d->intens.p, d->win_dev.p, d->rt_dev.p, v(d->n_obs),
+          v((int64_t)d->rt.size()), v(d->max_overlap),
+          l->arena.p, v(l->n_prec), v(l->n_frag), v(l->max_frag), v(l->min_frag), v(l->has_tol),
+          v(tol_bits)};
 }
 
 // A search, with use_graph: the first search of a (run, library, collection) runs
@@ -1101,6 +1111,7 @@ int launch_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandidat
   DeviceGuard dg(s->device);
   cudaStream_t st = s->o.stream ? (cudaStream_t)s->o.stream : s->stream;
   if (s->graph && c->done && graph_key(s, d, l, c) == s->graph_key) {
+    ADS_TRY(lib_ready_on(l, st));
     ADS_CUDA(cudaStreamWaitEvent(st, c->done, 0));
     c->pending = true;
     c->count = 0;

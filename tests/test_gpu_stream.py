@@ -57,3 +57,26 @@ def test_streamed_searches_match_serial(precision):
             assert n == len(ref["rank"])
             for c in COLS:
                 assert np.array_equal(outs[j % 2][c][:n].view(np.uint8), np.asarray(ref[c]).view(np.uint8)), (j, c)
+
+
+def test_graph_replay_after_library_replaced():
+    """use_graph: a library released and another built in its place (the handle may land
+    at the same address) is searched afresh, not through the old library's graph."""
+    cfg, run, libs = _libraries()
+    dia = DIAData.from_arrays(*(run[k] for k in RUN_KEYS), run["cycle"])
+    params = params_from(cfg.params_dict())
+    sel = PeakGroupSelection(params, verbose=False, use_graph=True)
+    cand = sel.new_candidates()
+    for j in (0, 1, 0):
+        la, tol = libs[j]
+        sl = SpecLibFlat.from_arrays(**la, precursor_rt_tolerance=tol)
+        ref = dict(zip(COLS, PeakGroupSelection(params, verbose=False).search(dia, sl).to_arrays()))
+        for _ in range(2):  # captured, then replayed
+            sel.search_into(dia, sl, cand)
+            n = cand.size()
+            got = {c: np.zeros(max(n, 1), np.float32 if c == "score" else np.uint64) for c in COLS}
+            cand.copy_out(got)
+            assert n == len(ref["rank"])
+            for c in COLS:
+                assert np.array_equal(got[c][:n].view(np.uint8), np.asarray(ref[c]).view(np.uint8)), (j, c)
+        del sl
