@@ -56,3 +56,18 @@ def test_both_arms_print_the_same_config():
     a = bench.bench_config(cfg, "bf16", 1)
     assert a == bench.bench_config(cfg, "bf16", 1)
     assert a["workload"].startswith("cfg3") and "per precursor" in a["rt_tolerance"]
+
+
+def test_host_copies_keep_shared_columns_shared():
+    """Columns that are one array (the synthetic library's m/z and library m/z) stay
+    one array after the host copy: the library upload then copies the m/z once, and
+    the bench's H2D count leaves the second name out."""
+    import torch
+
+    mz = torch.arange(5, dtype=torch.float32)
+    other = torch.ones(5)
+    out = bench.host_copies({"fragment_mz": mz, "fragment_mz_library": mz, "fragment_intensity": other},
+                            lambda t: t.clone())
+    assert out["fragment_mz"] is out["fragment_mz_library"]
+    assert out["fragment_intensity"] is not out["fragment_mz"]
+    assert torch.equal(out["fragment_mz"], mz) and out["fragment_mz"] is not mz
