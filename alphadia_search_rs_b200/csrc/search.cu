@@ -607,6 +607,7 @@ struct AdsSelection {
   ads::DevBuf<uint8_t> keep;
   ads::DevBuf<unsigned long long> work;
   ads::DevBuf<int> class_lists;
+  ads::DevBuf<unsigned int> class_hist;  // (class, fragment count) histogram, then cursors
   ads::DevBuf<int64_t> block_sums;
   ads::DevBuf<float> grow;  // warps' working sets of long-window launches
   ads::DevBuf<float> taps;  // kernel taps on the device, for half widths past kMaxHalf
@@ -693,6 +694,85 @@ __global__ void classify_kernel(int64_t P, const int* nf, const int* cs, const i
     if (b >= 0 && lane == leader) base = atomicAdd(counts + b, (unsigned)__popc(grp));
     base = __shfl_sync(kFull, base, leader);
     if (b >= 0) lists[(int64_t)b * P + base + __popc(grp & ((1u << lane) - 1u))] = (int)p;
+  }
+}
+
+// Class lists in order of decreasing fragment count (longest-processing-time first:
+// the warps that pull the last precursors of a launch get light ones, so the launch
+// ends on a short tail).  A counting sort over (class, fragment count): a histogram,
+// its exclusive scan in descending key order, then a scatter.  Keys above
+// kOrderKeys - 1 share the top bucket.
+constexpr int kOrderKeys = 256;
+
+__device__ __forceinline__ int precursor_class(const int* nf, const int* cs, const int* ce, int64_t p,
+                                               int n_cls, const LenClasses& cls, int* key) {
+  const int C = ce[p] - cs[p];
+  const int F = nf[p];
+  if (F == 0 || C <= 0) return -1;
+  int b = n_cls - 1;
+  for (int i = 0; i < n_cls - 1; ++i)
+    if (C <= cls.bound[i]) {
+      b = i;
+      break;
+    }
+  *key = min(F, kOrderKeys - 1);
+  return b;
+}
+
+__global__ void class_hist_kernel(int64_t P, const int* nf, const int* cs, const int* ce, int n_cls,
+                                  LenClasses cls, unsigned int* hist, int* cand_n) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x; p0 < P; p0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = p0 + threadIdx.x;
+    int b = -1, key = 0;
+    if (p < P) {
+      b = precursor_class(nf, cs, ce, p, n_cls, cls, &key);
+      if (b < 0) cand_n[p] = 0;
+    }
+    const int slot = b < 0 ? -1 : b * kOrderKeys + key;
+    const unsigned grp = __match_any_sync(kFull, slot);
+    if (slot >= 0 && lane == __ffs(grp) - 1) atomicAdd(hist + slot, (unsigned)__popc(grp));
+  }
+}
+
+// One block of kOrderKeys threads: per class, cursor[b][k] = precursors of class b with
+// a larger key; class_len[b] = the class's size.
+__global__ void __launch_bounds__(kOrderKeys) class_offsets_kernel(int n_cls, const unsigned int* hist,
+                                                                   unsigned int* cursor,
+                                                                   unsigned int* class_len) {
+  __shared__ unsigned int sh[kOrderKeys];
+  const int t = threadIdx.x;  // position in descending key order
+  const int k = kOrderKeys - 1 - t;
+  for (int b = 0; b < n_cls; ++b) {
+    const unsigned int v = hist[b * kOrderKeys + k];
+    sh[t] = v;
+    __syncthreads();
+    for (int o = 1; o < kOrderKeys; o <<= 1) {  // inclusive scan (Hillis-Steele)
+      const unsigned int add = t >= o ? sh[t - o] : 0u;
+      __syncthreads();
+      sh[t] += add;
+      __syncthreads();
+    }
+    cursor[b * kOrderKeys + k] = sh[t] - v;
+    if (t == kOrderKeys - 1) class_len[b] = sh[t];
+    __syncthreads();
+  }
+}
+
+__global__ void class_scatter_kernel(int64_t P, const int* nf, const int* cs, const int* ce, int n_cls,
+                                     LenClasses cls, unsigned int* cursor, int* lists) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x; p0 < P; p0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = p0 + threadIdx.x;
+    int b = -1, key = 0;
+    if (p < P) b = precursor_class(nf, cs, ce, p, n_cls, cls, &key);
+    const int slot = b < 0 ? -1 : b * kOrderKeys + key;
+    const unsigned grp = __match_any_sync(kFull, slot);
+    const int leader = __ffs(grp) - 1;
+    unsigned base = 0;
+    if (slot >= 0 && lane == leader) base = atomicAdd(cursor + slot, (unsigned)__popc(grp));
+    base = __shfl_sync(kFull, base, leader);
+    if (slot >= 0) lists[(int64_t)b * P + base + __popc(grp & ((1u << lane) - 1u))] = (int)p;
   }
 }
 
@@ -809,7 +889,13 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
   ADS_TRY(s->cand_score.reserve(Pn * k_out));
   ADS_TRY(s->cand_center.reserve(Pn * k_out));
   ADS_TRY(s->work.reserve(2 * kMaxClasses));  // work counters, then class lengths
-  if (n_cls > 1) ADS_TRY(s->class_lists.reserve(Pn * n_cls));
+  // precursors taken heaviest first when their fragment counts differ (class lists
+  // ordered by fragment count; a single class then gets a list too)
+  const bool order = std::min<int64_t>(prm.top_k_fragments, l->min_frag) <
+                     std::min<int64_t>(prm.top_k_fragments, l->max_frag);
+  const bool use_lists = n_cls > 1 || order;
+  if (use_lists) ADS_TRY(s->class_lists.reserve(Pn * n_cls));
+  if (order) ADS_TRY(s->class_hist.reserve(2 * kMaxClasses * kOrderKeys));
   const int64_t nb = (P + kScanBlock - 1) / kScanBlock;
   ADS_TRY(s->block_sums.reserve((size_t)nb));
   if (s->stats_on) {
@@ -916,7 +1002,20 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
   sa.stats = s->stats_on ? s->stats.p : nullptr;
   if (timed) ADS_CUDA(cudaEventRecord(s->stage_ev[1], st));
   unsigned int* class_len = reinterpret_cast<unsigned int*>(s->work.p + kMaxClasses);
-  if (n_cls > 1) {
+  if (order) {
+    const int cb = (int)std::min<int64_t>((P + 255) / 256, (int64_t)s->num_sms * 8);
+    unsigned int* hist = s->class_hist.p;
+    unsigned int* cursor = s->class_hist.p + kMaxClasses * kOrderKeys;
+    ADS_CUDA(cudaMemsetAsync(hist, 0, (size_t)n_cls * kOrderKeys * sizeof(unsigned int), st));
+    class_hist_kernel<<<cb, 256, 0, st>>>(P, s->nf.p, s->cs.p, s->ce.p, n_cls, cls, hist, s->cand_n.p);
+    ADS_LAUNCH_CHECK();
+    class_offsets_kernel<<<1, kOrderKeys, 0, st>>>(n_cls, hist, cursor, class_len);
+    ADS_LAUNCH_CHECK();
+    class_scatter_kernel<<<cb, 256, 0, st>>>(P, s->nf.p, s->cs.p, s->ce.p, n_cls, cls, cursor,
+                                             s->class_lists.p);
+    ADS_LAUNCH_CHECK();
+    launches += 3;
+  } else if (n_cls > 1) {
     const int cb = (int)std::min<int64_t>((P + 255) / 256, (int64_t)s->num_sms * 8);
     classify_kernel<<<cb, 256, 0, st>>>(P, s->nf.p, s->cs.p, s->ce.p, n_cls, cls,
                                          s->class_lists.p, class_len, s->cand_n.p);
@@ -947,8 +1046,8 @@ int enqueue_search(AdsSelection* s, const AdsDia* d, const AdsLib* l, AdsCandida
     ADS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nw * 32, smem));
     if (occ <= 0) return fail(ADS_ERR_INTERNAL, "search kernel cannot be resident");
     const int bps = s->o.blocks_per_sm > 0 ? std::min(s->o.blocks_per_sm, occ) : occ;
-    sa.list = n_cls > 1 ? s->class_lists.p + (int64_t)b * P : nullptr;
-    sa.list_len = n_cls > 1 ? class_len + b : nullptr;
+    sa.list = use_lists ? s->class_lists.p + (int64_t)b * P : nullptr;
+    sa.list_len = use_lists ? class_len + b : nullptr;
     sa.c_max = cmax_b;
     sa.ncell = ncell_b;
     sa.work = s->work.p + b;
@@ -1095,7 +1194,8 @@ std::vector<const void*> graph_key(const AdsSelection* s, const AdsDia* d, const
   std::memcpy(&tol_bits, &l->max_tol, sizeof(tol_bits));
   return {d, l, c, c->arena.p, s->nf.p, s->cs.p, s->ce.p, s->nwin.p, s->wins.p, s->fw.p,
           s->blo.p, s->bhi.p, s->keep.p, s->cand_n.p, s->cand_score.p, s->cand_center.p,
-          s->work.p, s->class_lists.p, s->block_sums.p, s->stats_on ? s->stats.p : nullptr,
+          s->work.p, s->class_lists.p, s->class_hist.p, s->block_sums.p,
+          s->stats_on ? s->stats.p : nullptr,
           d->intens_bf16.p, s->grow.p, s->taps.p,
           d->slice_starts.p, d->cycles.p, d->intens.p, d->win_dev.p, d->rt_dev.p, v(d->n_obs),
           v((int64_t)d->rt.size()), v(d->max_overlap),
